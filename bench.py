@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark: MRA log-likelihood evaluations per second on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3] [--precision fp64|mixed]
+    python bench.py --impl reference ...      # the reference's own CPU code on this host
+
+A step is one exact log-likelihood evaluation (prior + posterior pass over the
+whole partition tree) of a seeded synthetic configuration, with the partition,
+observations and all working buffers resident in HBM.  ``value`` is timed on the
+device with CUDA events recorded on the library's own stream; ``e2e`` times the
+same evaluation through the C ABI with the step's inputs (observation values y
+and theta) copied from pinned host memory and the result read back, every step.
+The multi-GPU form runs independent replicas (the path is not sharded: one
+likelihood evaluation fits one GPU), one process per GPU.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MRA loglik evals/sec at n=1M (mixed vs plain FP64, same GPU, ≤1e-6 rel err); fit wall-time"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "mra_ref_ext")
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-graph", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_name(cfg) -> str:
+    layout = {"uniform": "uniform", "mix70": "70% in 16 clusters + 30% uniform",
+              "mix10": "90% uniform + 10% in 16 clusters"}[cfg.layout]
+    return (f"{cfg.name}: n={cfg.n} locations on [0,1]^2 ({layout}), M={cfg.M}, J={cfg.J}, r={cfg.r}, "
+            f"nonstationary Matern nu={cfg.nu_x2}/2 with 9-RBF log-sigma/log-range fields")
+
+
+# ---------------------------------------------------------------------------
+# data
+# ---------------------------------------------------------------------------
+def make_problem(cfg, with_pred=False):
+    from nonstationary_mra_b200 import partition, synth
+    rng = np.random.Generator(np.random.PCG64(cfg.seed))
+    xy, pred = synth.locations(cfg, rng)
+    theta = synth.true_theta(cfg, rng)
+    md = synth.model_from_theta(theta, cfg.nu_x2)
+    st = partition.build_by_program(xy[0], xy[1], np.zeros(cfg.n), cfg.J, cfg.M, cfg.r, math.exp(1) / 100,
+                                    pred[0] if with_pred else None, pred[1] if with_pred else None,
+                                    distance=2, all_lon=xy[0], all_lat=xy[1])
+    return xy, pred, theta, md, st
+
+
+def draw_values(ctx, st, seed):
+    """y from the MRA prior at the true parameters (standard normals from PCG64)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    z_int = rng.standard_normal(st.n_interior * st.r)
+    z_obs = rng.standard_normal(st.n_obs)
+    ctx.set_theta()
+    return ctx.sample_prior(z_int, z_obs)
+
+
+# ---------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()) if rows else None}
+
+
+def fp64_peak_tflops():
+    """cuBLAS DGEMM throughput (torch.matmul in float64), best of 5 at 8192^3."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    best = 0.0
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def measured_peaks():
+    try:
+        return json.load(open(PEAKS_FILE))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own code on a bounded sample, scaled by FLOPs
+# ---------------------------------------------------------------------------
+def cpu_sample_config(cfg):
+    from nonstationary_mra_b200 import synth
+    # same generator and model, 1/64 of the points with the tree two levels
+    # shallower (same mean observations per finest region)
+    return synth.Config(cfg.name + "-cpu-sample", cfg.n // 64, cfg.M - 3, cfg.J, cfg.r, cfg.nu_x2, 0, cfg.layout,
+                        cfg.range_sd, cfg.seed + 1000)
+
+
+def canonical_flops(st):
+    """Algorithmic FLOPs of one log-likelihood (same count as the library's plan)."""
+    J, M, R = st.J, st.M, float(st.r)
+    total = 0.0
+    for m in range(M - 1):
+        cnt = float(J ** m)
+        total += 2 * cnt * R ** 3 * (m * (m - 1) / 2 + m + 1.0 / 6)
+        total += 2 * cnt * (R ** 3 * (1.0 / 3 + m + m * (m - 1) / 2) + R * R * (0.5 + m))
+    Lv = M - 1
+    n = np.diff(st.obs_offset).astype(np.float64)
+    n = n[n > 0]
+    total += 2 * np.sum(R * R * n * Lv * (Lv - 1) / 2 + Lv * R * R * n / 2 + Lv * R * n * n / 2 + n ** 3 / 6 +
+                        n * n / 2 + Lv * n * n * R / 2 + Lv * R * n + Lv * R * R * n / 2 +
+                        Lv * (Lv - 1) / 2 * R * R * n)
+    return float(total)
+
+
+def run_cpu_reference(cfg, reps, warmup, ctx_factory=None):
+    """Times Approximation::likelihood() of the reference (compiled from its own
+    sources, oracle/_ref) on the bounded sample, all host threads.  Falls back to
+    the numpy restatement of the oracle when the reference binary is absent."""
+    from nonstationary_mra_b200 import refio, synth
+    sc = cpu_sample_config(cfg)
+    xy, _, theta, md, st = make_problem(sc)
+    f_sample = canonical_flops(st)
+    cores = os.cpu_count() or 1
+    tmp = tempfile.mkdtemp(prefix="mra_cpu_")
+    try:
+        y = np.zeros(sc.n)
+        if ctx_factory is not None:
+            ctx = ctx_factory(st, md)
+            y_st = draw_values(ctx, st, sc.seed + 7)
+            ctx.close()
+            y[st.obs_index] = y_st
+        synth.write_case(tmp, sc, xy, y, np.zeros((2, 0)), theta)
+        if os.path.exists(REF_BIN):
+            X = refio.parse_parameters(os.path.join(tmp, "ext_parameters"))
+            env = dict(os.environ, OMP_NUM_THREADS=str(cores), OPENBLAS_NUM_THREADS="1",
+                       **{k: str(v) for k, v in X.items()})
+            res = subprocess.run([REF_BIN, "--reps", str(reps + warmup)], cwd=tmp, env=env, capture_output=True,
+                                 text=True, timeout=1800)
+            if res.returncode != 0:
+                raise RuntimeError(res.stdout[-1000:] + res.stderr[-1000:])
+            secs = [float(tok.split("=")[1]) for line in res.stdout.splitlines() if line.startswith("ORACLE rep=")
+                    for tok in line.split() if tok.startswith("likelihood_seconds=")]
+            secs = secs[warmup:]
+            kind, used = "reference", cores
+        else:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import mra_oracle as oracle
+            ost, omd, _ = oracle.load_case(tmp, mode="likelihood")
+            secs = []
+            for i in range(reps + warmup):
+                t0 = time.perf_counter()
+                oracle.loglik(ost, omd)
+                if i >= warmup:
+                    secs.append(time.perf_counter() - t0)
+            kind, used = "port", 1
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"secs": secs, "f_sample": f_sample, "kind": kind, "cores": used, "sample": sc, "n_obs": st.n_obs}
+
+
+def reference_arm(args):
+    from nonstationary_mra_b200 import synth
+    cfg = synth.CONFIGS[args.config]
+    _, _, _, _, st_full = make_problem(cfg)
+    f_full = canonical_flops(st_full)
+    r = run_cpu_reference(cfg, max(args.steps, 1), max(args.warmup, 0))
+    t = statistics.median(r["secs"])
+    value = 1.0 / (t * f_full / r["f_sample"])
+    sc = r["sample"]
+    sample = (f"{sc.n} points, M={sc.M}, J={sc.J}, r={sc.r} (same generator), one likelihood() per step, "
+              f"scaled to the {cfg.name} workload by algorithmic FLOPs ({f_full:.3e} / {r['f_sample']:.3e})")
+    line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": len(r["secs"]),
+            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(cfg), "parallelism": "cpu", "sample_seconds_median": t},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": r["cores"], "kind": r["kind"],
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from nonstationary_mra_b200 import api, synth
+
+    torch.cuda.set_device(local)
+    api.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    cfg = synth.CONFIGS[args.config]
+    t_setup = time.perf_counter()
+    xy, pred, theta, md, st = make_problem(cfg)
+    ctx = api.Context(st, md, precision=args.precision)
+    y = draw_values(ctx, st, cfg.seed + 7)
+    ctx.set_obs_values(y)
+    ctx.set_theta()
+    setup_s = time.perf_counter() - t_setup
+
+    for _ in range(max(args.warmup, 0)):
+        ctx.loglik()
+    if not args.no_graph:
+        ctx.capture_graph()
+        ctx.loglik()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    # device-resident timing
+    barrier()
+    with ClockSampler(local) as clk:
+        ctx.timer_start()
+        for _ in range(args.steps):
+            d, ll = ctx.loglik()
+        ms = ctx.timer_stop()
+    barrier()
+    stats = ctx.stats()
+
+    # end to end through the C ABI: pinned y -> device, theta -> device, evaluate, result -> host
+    y_pinned = torch.from_numpy(y.copy()).pin_memory()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        ctx.set_obs_values_ptr(y_pinned.data_ptr())
+        ctx.set_theta()
+        d2, ll2 = ctx.loglik()
+    ms_e2e = ctx.timer_stop()
+    barrier()
+
+    t_max = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms, ms_e2e = t_max.tolist()
+    value = world * args.steps / (ms * 1e-3)
+    e2e = world * args.steps / (ms_e2e * 1e-3)
+
+    # roofline of the dominant launch of one evaluation
+    launches = stats["launches"]
+    dom = max(launches, key=lambda l: l["ms"])
+    achieved = dom["flop"] / (dom["ms"] * 1e-3) / 1e12
+    peak = fp64_peak_tflops() if rank == 0 else None
+    traffic = None
+    if os.path.exists(TRAFFIC_FILE):
+        tj = json.load(open(TRAFFIC_FILE))
+        traffic = tj.get(f"{args.config}:{args.precision}:{dom['kernel']}:{dom['level']}")
+    ctx.close()
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            r = run_cpu_reference(cfg, 3, 1, ctx_factory=lambda s, m: api.Context(s, m))
+            t = statistics.median(r["secs"])
+            f_full = stats["flop_last"]
+            sc = r["sample"]
+            cpu = {"value": 1.0 / (t * f_full / r["f_sample"]), "unit": "evals/s", "cores": r["cores"],
+                   "kind": r["kind"],
+                   "sample": (f"{sc.n} points, M={sc.M}, J={sc.J}, r={sc.r} (same generator): median of "
+                              f"{len(r['secs'])} likelihood() runs = {t:.3f} s, scaled to this workload by "
+                              f"algorithmic FLOPs ({f_full:.3e} / {r['f_sample']:.3e})")}
+        except Exception as exc:  # reported, never silently replaced
+            cpu = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {exc}"[:300]}
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "mixed-f32tc-f64",
+        "data": "synthetic (seeded, y drawn from the MRA prior)",
+        "config": {"workload": workload_name(cfg), "precision": args.precision, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (whole tree resident in HBM, no flush needed)",
+                   "cuda_graph": not args.no_graph, "loglik": ll, "d": d, "n_obs": st.n_obs,
+                   "setup_seconds": setup_s, "device_gb": stats["bytes_device"] / 1e9,
+                   "flop_per_eval": stats["flop_last"],
+                   "stage_ms": {k: stats[k] for k in ("ms_fields", "ms_prior", "ms_finest", "ms_posterior")}},
+        "roofline": {"bound": "tensor", "kernel": f"{dom['kernel']}(level {dom['level']})",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
+                                    "MEASURED_PEAKS.json)"},
+        "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": 8 * st.n_obs + 16 * 8 + 8 * 18,
+                "d2h_bytes_per_step": 8 + 16},
+        "gpu_launches": stats["kernel_launches"] * args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

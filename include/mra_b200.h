@@ -1,0 +1,205 @@
+/*
+ * nonstationary_mra_b200 -- C ABI of the B200 (sm_100a) MRA hot path.
+ *
+ * This boundary replaces, for one GPU, the reference's
+ *   Approximation::likelihood()      include/class_approximation.hpp:53
+ *                                    (src/class_approximation.cpp:466-470)
+ *   Approximation::predict()         include/class_approximation.hpp:56
+ *                                    (src/class_approximation-predict.cpp:15-200)
+ *   evaluate_*covariance()           include/evaluate_covariance.hpp:25,47,71,88
+ *   Nonstationary_covariance::get_*  include/class_nonstationary_covariance.hpp:55-64
+ * The partition / knots / observation arrays that the reference keeps in
+ * `Partition` (include/class_partition.hpp:26-61) are passed in once as flat
+ * arrays (mra_structure) and stay resident in HBM; each likelihood evaluation
+ * then only takes the covariance parameters (mra_theta).
+ *
+ * Conventions: plain pointers and sizes, host memory unless a name says
+ * otherwise, column-major matrices as in the reference.  Every function
+ * returns an mra_status; nothing exits the process (the reference prints and
+ * calls exit(); the drop-in C++ host maps statuses to that behaviour).
+ * A context is single-threaded and stream-ordered: do not call into the same
+ * mra_ctx from two threads at once.
+ */
+#ifndef MRA_B200_H
+#define MRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MRA_OK = 0,
+    MRA_ERR_ARG = 1,       /* invalid argument or inconsistent structure */
+    MRA_ERR_CUDA = 2,      /* CUDA runtime error (message in mra_last_error) */
+    MRA_ERR_OOM = 3,       /* device allocation failed */
+    MRA_ERR_NOT_SPD = 4,   /* a Cholesky pivot was not positive (region in mra_stats) */
+    MRA_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+    MRA_ERR_STATE = 6,     /* call out of order (e.g. predict without predictions) */
+    MRA_ERR_NO_DEVICE = 7  /* no usable sm_100 device */
+} mra_status;
+
+/* Distance between points (coordinates are 3 doubles per point, SoA). */
+typedef enum {
+    MRA_DIST_CHORDAL = 0,      /* (x,y,z) on the unit sphere, |p-q| * dist_scale  (CHORDAL_DISTANCE_FLAG=true)  */
+    MRA_DIST_GREAT_CIRCLE = 1, /* (lon,lat) degrees, arccos(...) * dist_scale      (CHORDAL_DISTANCE_FLAG=false) */
+    MRA_DIST_EUCLID2D = 2      /* (x,y) planar, |p-q| * dist_scale                  (extension)                   */
+} mra_distance;
+
+typedef enum {
+    MRA_BASIS_WENDLAND = 0,    /* (1-d)^6 (35d^2+18d+3)/3 for d<1 (reference)      */
+    MRA_BASIS_GAUSSIAN = 1     /* exp(-d^2/2) (extension)                          */
+} mra_basis;
+
+typedef enum {
+    MRA_PRECISION_FP64 = 0,    /* plain FP64 path                                   */
+    MRA_PRECISION_MIXED = 1    /* FP32 covariance + tensor-core trailing updates,
+                                  FP64 diagonal-block Cholesky and accumulations   */
+} mra_precision;
+
+/* Partition tree, knots, observations and (optionally) prediction locations.
+ * Interior regions 0..n_interior-1 are levels 0..M-2 in heap order (children
+ * of region i are i*J+1..i*J+J, class_approximation.cpp:36-43).  Finest region
+ * k (reference index n_interior+k) has parent finest_parent[k]; the finest
+ * children of one parent must be a contiguous range, as the reference assumes
+ * (childrenStart/childrenEnd, class_partition.cpp:740-770).                    */
+typedef struct {
+    int32_t J;                     /* NUM_PARTITIONS_J (2 or 4)                     */
+    int32_t M;                     /* NUM_LEVELS_M (>= 2)                           */
+    int32_t r;                     /* knots per interior region                     */
+    int32_t reserved;
+    uint64_t n_interior;           /* (J^(M-1)-1)/(J-1)                             */
+    uint64_t n_finest;
+    const uint64_t* finest_parent; /* [n_finest]                                     */
+    const double* knots;           /* [3][n_interior*r]: coordinate c of knot q of
+                                      region i at knots[c*n_interior*r + i*r + q]   */
+    const uint64_t* obs_offset;    /* [n_finest+1] CSR offsets into observations     */
+    const double* obs;             /* [3][n_obs]                                     */
+    const double* obs_value;       /* [n_obs] residuals y (knotsResidual)            */
+    const uint64_t* pred_offset;   /* [n_finest+1] or NULL                           */
+    const double* pred;            /* [3][n_pred] or NULL                            */
+} mra_structure;
+
+/* One nonstationary log-field: log f(s) = intercept + sum_k w_k basis(|s-c_k|/len). */
+typedef struct {
+    uint64_t n_basis;
+    const double* centers;         /* [3][n_basis] in the point coordinate system    */
+    const double* weights;         /* [n_basis]                                      */
+    double intercept;
+} mra_field;
+
+typedef struct {
+    int32_t nonstationary;         /* NONSTATIONARY_FLAG                             */
+    int32_t distance;              /* mra_distance                                   */
+    int32_t nu_x2;                 /* 2*nu: 1 = exponential (reference), 3 = Matern 3/2 */
+    int32_t basis;                 /* mra_basis                                      */
+    double prefactor_exp;          /* e in (b1 b2 / bbar^2)^e: 1.5 (reference), 1.0 (d=2) */
+    double dist_scale;             /* 6371 (reference) or 1                          */
+    double basis_len;              /* WENDLAND_LEN or Gaussian width                 */
+    mra_field field[3];            /* sill (sigma^2), range (beta), nugget (tau^2)   */
+} mra_model;
+
+/* Per-evaluation parameters: the six arguments of Approximation's constructor
+ * (include/class_approximation.hpp:46) plus optional overrides of the field
+ * intercepts/weights (the extension's 19-dimensional theta).                  */
+typedef struct {
+    double sill, range, nugget;                     /* stationary model          */
+    double sill_scale, range_scale, nugget_scale;   /* nonstationary scales      */
+    const double* weights[3];      /* NULL: keep the model's weights             */
+    const double* intercepts;      /* NULL or [3]: replace the model's intercepts */
+} mra_theta;
+
+/* Kernel kinds in mra_stats.timed_kind. */
+typedef enum {
+    MRA_KERNEL_FIELDS = 0,         /* sigma^2 / beta / tau^2 at every point          */
+    MRA_KERNEL_PRIOR_LEVEL = 1,    /* prior of one interior level (timed_level = m)  */
+    MRA_KERNEL_FINEST = 2,         /* prior of the finest level                      */
+    MRA_KERNEL_POSTERIOR_LEVEL = 3,/* posterior of one interior level                */
+    MRA_KERNEL_REDUCE = 4,         /* final log-likelihood sum                       */
+    MRA_KERNEL_PREDICT = 5         /* prediction                                     */
+} mra_kernel_kind;
+
+#define MRA_MAX_TIMED 40
+
+typedef struct {
+    double d;                      /* the reference's internal loglikelihood after
+                                      likelihood(): sum of log-dets and quadratic forms */
+    double loglik;                 /* -0.5 (d + n log(2*3.14159265359))          */
+    double ms_total;               /* device time of the last evaluation          */
+    double ms_fields, ms_prior, ms_finest, ms_posterior, ms_predict;
+    double flop_last;              /* algorithmic FLOPs of the last evaluation    */
+    uint64_t bytes_device;         /* device memory held by the context           */
+    int64_t bad_region;            /* region of the last MRA_ERR_NOT_SPD, else -1 */
+    int32_t kernel_launches;       /* kernels launched by the last evaluation     */
+    int32_t graph_replays;
+    int32_t n_timed;               /* launches of the last evaluation, in order   */
+    int32_t timed_kind[MRA_MAX_TIMED];   /* mra_kernel_kind                        */
+    int32_t timed_level[MRA_MAX_TIMED];  /* tree level for per-level kernels, else -1 */
+    double timed_ms[MRA_MAX_TIMED];      /* device time of each launch (CUDA events) */
+    double timed_flop[MRA_MAX_TIMED];    /* algorithmic FLOPs of each launch          */
+} mra_stats;
+
+typedef struct mra_ctx mra_ctx;
+
+/* Uploads the structure and model; allocates every device buffer up front. */
+mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precision, mra_ctx** out);
+mra_status mra_destroy(mra_ctx* ctx);
+
+/* Sets the parameters for the next evaluations (a 1-10 word host->device copy). */
+mra_status mra_set_theta(mra_ctx* ctx, const mra_theta* theta);
+
+/* Replaces the observation values y (n_obs doubles, host memory). */
+mra_status mra_set_obs_values(mra_ctx* ctx, const double* y);
+
+/* Prior + posterior: Approximation::likelihood() in likelihood mode.
+ * d_out / loglik_out may be NULL. */
+mra_status mra_loglik(mra_ctx* ctx, double* d_out, double* loglik_out);
+
+/* Prior + posterior + prediction: Approximation::likelihood() then predict() in
+ * prediction mode.  mean/var: n_pred doubles each, in finest-region order (the
+ * order of dump_prediction_result, class_approximation.cpp:493-535). */
+mra_status mra_predict(mra_ctx* ctx, double* mean, double* var);
+
+/* Captures prior->posterior into a CUDA graph; later mra_loglik calls replay it. */
+mra_status mra_capture_graph(mra_ctx* ctx);
+
+mra_status mra_get_stats(const mra_ctx* ctx, mra_stats* out);
+
+/* Draws y from the MRA prior at the current theta:
+ * y = sum_j U_{obs,j}^T z_{a_j} + L_Sigma z_k, z_interior [n_interior*r],
+ * z_obs [n_obs] standard normals given by the caller (host memory). */
+mra_status mra_sample_prior(mra_ctx* ctx, const double* z_interior, const double* z_obs, double* y_out);
+
+/* Covariance blocks with the reference's layout out[i1*n2+i2]
+ * (evaluate_covariance.cpp:56-313), computed on the device.  p1/p2 are
+ * [3][n] coordinates; the fields come from the model and theta.  Cross block
+ * when self == 0, symmetric self block with sigma^2+tau^2 on the diagonal
+ * when self != 0 (then p2/n2 are ignored). */
+mra_status mra_eval_covariance(const mra_model* m, const mra_theta* theta, const double* p1, uint64_t n1,
+                               const double* p2, uint64_t n2, int32_t self, double* out);
+
+/* sigma^2, beta, tau^2 at n points (Nonstationary_covariance::get_* times the
+ * scales), computed on the device.  out: [3][n]. */
+mra_status mra_eval_fields(const mra_model* m, const mra_theta* theta, const double* p, uint64_t n,
+                           double* out);
+
+/* Selects the CUDA device that the calling thread's next mra_create uses
+ * (one process per GPU: call it with the local rank before mra_create). */
+mra_status mra_set_device(int32_t device);
+
+/* Device-side timer on the context's stream: mra_timer_stop returns the device
+ * time between the two calls, covering every copy and kernel the context issued
+ * in between (CUDA events; waits for the stream). */
+mra_status mra_timer_start(mra_ctx* ctx);
+mra_status mra_timer_stop(mra_ctx* ctx, double* ms);
+
+/* Text of the last error on this thread. */
+const char* mra_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MRA_B200_H */
