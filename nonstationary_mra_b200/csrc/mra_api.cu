@@ -174,15 +174,24 @@ mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 }
 
 // Issues one evaluation on the context's stream: every launch of the plan
-// (plus prediction) bracketed by its own pair of timing events.
+// (plus prediction) bracketed by its own pair of timing events.  The events are
+// recorded as external nodes so that they still time each launch when the
+// sequence is replayed from a captured CUDA graph.
+cudaError_t record(cudaEvent_t e, cudaStream_t st, bool capturing) {
+    return capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+}
+
 mra_status run_eval(mra_ctx* c, bool predict) {
     cudaStream_t st = c->stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CU(cudaStreamIsCapturing(st, &cap));
+    const bool capturing = cap == cudaStreamCaptureStatusActive;
     CU(cudaMemsetAsync(c->t.queue, 0, 4 * sizeof(int), st));
     CU(cudaMemsetAsync(c->t.err, 0, 4 * sizeof(int), st));
     const long np_all = c->n_int * c->r + c->n_obs + c->n_pred;
     int i = 0;
     for (const auto& l : c->plan) {
-        CU(cudaEventRecord(c->tev[2 * i], st));
+        CU(record(c->tev[2 * i], st, capturing));
         switch (l.kind) {
             case MRA_KERNEL_FIELDS:
                 launch_fields(c->geom, c->fp, c->t.pts.c0, c->t.pts.c1, c->t.pts.c2, np_all,
@@ -196,13 +205,13 @@ mra_status run_eval(mra_ctx* c, bool predict) {
                 break;
             case MRA_KERNEL_REDUCE: launch_reduce(c->t, c->d_result, st); break;
         }
-        CU(cudaEventRecord(c->tev[2 * i + 1], st));
+        CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
     }
     if (predict) {
-        CU(cudaEventRecord(c->tev[2 * i], st));
+        CU(record(c->tev[2 * i], st, capturing));
         launch_predict(c->geom, c->t, c->grid, st);
-        CU(cudaEventRecord(c->tev[2 * i + 1], st));
+        CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
     }
     CU(cudaGetLastError());
