@@ -195,6 +195,32 @@ mra_status mra_set_device(int32_t device);
 mra_status mra_timer_start(mra_ctx* ctx);
 mra_status mra_timer_stop(mra_ctx* ctx, double* ms);
 
+/* Allocation-free covariance blocks.  No counterpart in the reference.
+ *
+ * Same result and layout as mra_eval_covariance (out[i1*n2+i2]), for callers
+ * that cannot let this library allocate device memory: programs that give all
+ * device memory to their own pool or arena, and loops that cannot afford the
+ * device-wide synchronisation of cudaMalloc/cudaFree on every call.  Inputs and
+ * output are the caller's DEVICE buffers: p1_dev [3][n1] and p2_dev [3][n2]
+ * coordinates, out_dev n1*n2 doubles (n1*n1 when self != 0; p2_dev/n2 ignored).
+ * The model's basis tables and theta are read from host memory as elsewhere.
+ * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default stream)
+ * and the call returns without waiting for it.
+ *
+ * Scratch lives in one fixed array in device global memory, held by every GPU
+ * that loads the library until the process exits; limits: n1 + n2 <=
+ * MRA_STATIC_MAX_POINTS points and <= MRA_STATIC_MAX_BASIS basis functions per
+ * field, larger requests fail with MRA_ERR_ARG.  The first call on a device
+ * looks up that array's device address (once per device, with the device
+ * current); make that first call before any stream capture.  Every call uses
+ * the same array and overwrites all of it that it reads, so calls that overlap
+ * on the GPU (other streams, other host threads) race with each other:
+ * serialize them. */
+#define MRA_STATIC_MAX_POINTS 32768
+#define MRA_STATIC_MAX_BASIS 1024
+mra_status mra_eval_covariance_static(const mra_model* m, const mra_theta* theta, const double* p1_dev, uint64_t n1,
+                                      const double* p2_dev, uint64_t n2, int32_t self, double* out_dev, void* stream);
+
 /* Text of the last error on this thread. */
 const char* mra_last_error(void);
 

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmra_b200.so")
 
-CU_SOURCES = ["mra_kernels.cu", "mra_api.cu"]
+CU_SOURCES = ["mra_kernels.cu", "mra_api.cu", "mra_static.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

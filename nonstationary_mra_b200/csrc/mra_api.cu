@@ -41,6 +41,8 @@ struct DevBuf {
 
 }  // namespace
 
+void mra::set_last_error(const char* msg) { g_last_error = msg; }
+
 struct mra_ctx {
     int device = 0;
     int precision = 0;

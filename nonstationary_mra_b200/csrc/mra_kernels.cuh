@@ -78,6 +78,9 @@ struct FieldParams {
     const double* weights[3];  // [nb]
 };
 
+// Sets the text returned by mra_last_error() on this thread.
+void set_last_error(const char* msg);
+
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
 void launch_prior_level(const Geom& g, const DevTree& t, int m, int grid, cudaStream_t st);
