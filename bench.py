@@ -44,7 +44,7 @@ def parse_args():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    p.add_argument("--config", default="c3", choices=["c1", "c2", "c2s", "c3"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-graph", action="store_true")

@@ -48,6 +48,9 @@ CONFIGS = {
     "c2": Config("c2", 262144, 8, 4, 64, 1, 16384, "mix70", 0.3, 2),
     # large mixed-precision run (read as 90% uniform + 10% clustered), nu = 3/2
     "c3": Config("c3", 1048576, 10, 4, 64, 3, 65536, "mix10", 0.5, 3),
+    # c2's layout at a quarter of the points and one level less: the size used for
+    # full ncu captures (about 2 GB resident)
+    "c2s": Config("c2s", 65536, 7, 4, 64, 1, 4096, "mix70", 0.3, 4),
 }
 
 RBF_CENTERS_1D = np.array([1.0 / 6, 0.5, 5.0 / 6])
