@@ -115,10 +115,11 @@ typedef struct {
 typedef enum {
     MRA_KERNEL_FIELDS = 0,         /* sigma^2 / beta / tau^2 at every point          */
     MRA_KERNEL_PRIOR_LEVEL = 1,    /* prior of one interior level (timed_level = m)  */
-    MRA_KERNEL_FINEST = 2,         /* prior of the finest level                      */
+    MRA_KERNEL_FINEST = 2,         /* finest level + level M-2 posterior, per sibling group */
     MRA_KERNEL_POSTERIOR_LEVEL = 3,/* posterior of one interior level                */
     MRA_KERNEL_REDUCE = 4,         /* final log-likelihood sum                       */
-    MRA_KERNEL_PREDICT = 5         /* prediction                                     */
+    MRA_KERNEL_PREDICT = 5,        /* prediction                                     */
+    MRA_KERNEL_CONVERT = 6         /* FP32 -> FP64 widening between the mixed stages */
 } mra_kernel_kind;
 
 #define MRA_MAX_TIMED 40
@@ -129,7 +130,8 @@ typedef struct {
     double loglik;                 /* -0.5 (d + n log(2*3.14159265359))          */
     double ms_total;               /* device time of the last evaluation          */
     double ms_fields, ms_prior, ms_finest, ms_posterior, ms_predict;
-    double flop_last;              /* algorithmic FLOPs of the last evaluation    */
+    double flop_last;              /* FLOPs of the algorithm run by the last evaluation */
+    double flop_reference;         /* FLOPs of the reference's algorithm on the same tree */
     uint64_t bytes_device;         /* device memory held by the context           */
     int64_t bad_region;            /* region of the last MRA_ERR_NOT_SPD, else -1 */
     int32_t kernel_launches;       /* kernels launched by the last evaluation     */

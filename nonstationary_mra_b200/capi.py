@@ -52,12 +52,14 @@ class mra_theta(C.Structure):
 class mra_stats(C.Structure):
     _fields_ = [("d", C.c_double), ("loglik", C.c_double), ("ms_total", C.c_double), ("ms_fields", C.c_double),
                 ("ms_prior", C.c_double), ("ms_finest", C.c_double), ("ms_posterior", C.c_double),
-                ("ms_predict", C.c_double), ("flop_last", C.c_double), ("bytes_device", C.c_uint64),
+                ("ms_predict", C.c_double), ("flop_last", C.c_double), ("flop_reference", C.c_double),
+                ("bytes_device", C.c_uint64),
                 ("bad_region", C.c_int64), ("kernel_launches", C.c_int32), ("graph_replays", C.c_int32),
                 ("n_timed", C.c_int32), ("timed_kind", C.c_int32 * 40), ("timed_level", C.c_int32 * 40),
                 ("timed_ms", C.c_double * 40), ("timed_flop", C.c_double * 40)]
 
-KERNEL_NAMES = {0: "fields", 1: "prior_level", 2: "finest", 3: "posterior_level", 4: "reduce", 5: "predict"}
+KERNEL_NAMES = {0: "fields", 1: "prior_level", 2: "finest_group", 3: "posterior_level", 4: "reduce", 5: "predict",
+                6: "convert"}
 
 
 # (name, restype, argtypes) of every exported entry point of include/mra_b200.h

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -48,45 +49,50 @@ struct mra_ctx {
     int precision = 0;
     int sms = 0;
     int grid = 0;  // CTAs per region-kernel launch
-    int J = 0, M = 0, r = 0, L = 0;
+    int J = 0, M = 0, r = 0, L = 0, tf = 0;
     long n_int = 0, n_fin = 0, n_obs = 0, n_pred = 0;
     Geom geom{};
     FieldParams fp{};
-    DevTree t{};
+    DevTree<double> td{};
+    DevTree<float> tf32{};
     std::vector<DevBuf> bufs;
     size_t bytes = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8]{};
-    cudaEvent_t tev[2 * MRA_MAX_TIMED]{};   // start/stop of every launch
+    cudaEvent_t tev[2 * MRA_MAX_TIMED]{};  // start/stop of every launch
     struct Launch {
         int kind, level;
         double flop;
     };
-    std::vector<Launch> plan;               // launches of one log-likelihood, in order
+    std::vector<Launch> plan;  // launches of one log-likelihood, in order
     double flop_predict_launch = 0;
     int n_timed = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
-    double* d_theta = nullptr;  // 9 doubles
+    double* d_theta = nullptr;  // 16 doubles
     double* d_weights[3]{};
     long nb[3]{};
     std::vector<double> model_weights[3];
     double model_intercept[3]{};
     double* d_result = nullptr;  // [0] d
-    double flop_loglik = 0, flop_predict = 0;
+    double flop_loglik = 0, flop_reference = 0;
+    int64_t u_total = 0;
     mra_stats stats{};
     int last_launches = 0;
     bool have_pred = false;
 
-    template <typename T>
-    T* alloc(size_t count, cudaError_t* err) {
+    void* alloc_bytes(size_t bytes_, cudaError_t* err) {
         DevBuf b;
-        b.bytes = std::max<size_t>(count * sizeof(T), 16);
+        b.bytes = std::max<size_t>(bytes_, 16);
         *err = cudaMalloc(&b.p, b.bytes);
         if (*err != cudaSuccess) return nullptr;
         bufs.push_back(b);
         bytes += b.bytes;
-        return static_cast<T*>(b.p);
+        return b.p;
+    }
+    template <typename T>
+    T* alloc(size_t count, cudaError_t* err) {
+        return static_cast<T*>(alloc_bytes(count * sizeof(T), err));
     }
     ~mra_ctx() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -127,92 +133,164 @@ mra_status check_model(const mra_model* m) {
     return MRA_OK;
 }
 
-// Algorithmic FLOPs (2 per multiply-add; symmetric products counted once) of
-// every launch of one log-likelihood, from the realised region sizes.  The
-// per-region multiply-add counts are the canonical ones of the MRA:
-//   prior, level m:     r^3 [m(m-1)/2 + m/2 + m/2 + 1/6]
-//   posterior, level m: r^3 [1/3 + m/2 + m/2 + m(m-1)/2] + r^2 (1/2 + m)
-//   finest region, n observations, L = M-1 ancestors:
-//     r^2 n L(L-1)/2 + L r^2 n/2 + L r n^2/2 + n^3/6 + n^2/2 + L n^2 r/2   (finest kernel)
-//     L r n + L r^2 n/2 + L(L-1)/2 r^2 n     (w~ and A~ products; formed by the
-//                                              level M-2 posterior kernel here)
-void make_plan(mra_ctx* c, const std::vector<int64_t>& nfin) {
-    const int J = c->J, M = c->M;
-    const double R = c->r, Lv = M - 1;
-    double fields = 0;
-    for (int f = 0; f < 3; ++f) fields += (double)c->nb[f];
-    c->plan.clear();
-    c->plan.push_back({MRA_KERNEL_FIELDS, -1,
-                       (double)(c->n_int * c->r + c->n_obs + c->n_pred) * (fields * 12 + 8)});
-    for (int m = 0; m <= M - 2; ++m) {
-        double cnt = std::pow((double)J, m), mm = m;
-        c->plan.push_back({MRA_KERNEL_PRIOR_LEVEL, m,
-                           2 * cnt * R * R * R * (mm * (mm - 1) / 2 + mm / 2 + mm / 2 + 1.0 / 6)});
-    }
-    double fin = 0, agg = 0;
-    for (int64_t n64 : nfin) {
-        double n = (double)n64;
-        if (n == 0) continue;
-        fin += R * R * n * Lv * (Lv - 1) / 2 + Lv * R * R * n / 2 + Lv * R * n * n / 2 + n * n * n / 6 + n * n / 2 +
-               Lv * n * n * R / 2;
-        agg += Lv * R * n + Lv * R * R * n / 2 + Lv * (Lv - 1) / 2 * R * R * n;
-    }
-    c->plan.push_back({MRA_KERNEL_FINEST, M - 1, 2 * fin});
-    for (int m = M - 2; m >= 0; --m) {
-        double cnt = std::pow((double)J, m), mm = m;
-        double f = cnt * (R * R * R * (1.0 / 3 + mm / 2 + mm / 2 + mm * (mm - 1) / 2) + R * R * (0.5 + mm));
-        if (m == M - 2) f += agg;
-        c->plan.push_back({MRA_KERNEL_POSTERIOR_LEVEL, m, 2 * f});
-    }
-    c->plan.push_back({MRA_KERNEL_REDUCE, -1, (double)(c->n_int + c->n_fin)});
-    c->flop_loglik = 0;
-    for (auto& l : c->plan) c->flop_loglik += l.flop;
-}
-
 mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
     if (bytes == 0) return MRA_OK;
     CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
     return MRA_OK;
 }
 
-// Issues one evaluation on the context's stream: every launch of the plan
-// (plus prediction) bracketed by its own pair of timing events.  The events are
-// recorded as external nodes so that they still time each launch when the
-// sequence is replayed from a captured CUDA graph.
+// Host-side description of the tree used for sizing, scheduling and FLOP counts.
+struct HostTree {
+    std::vector<int64_t> nfin, npred, obs_off, pred_off, fin_anc, fin_order, lsig_off, pc_off;
+    std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi;
+    std::vector<int8_t> factored;
+};
+
+// Algorithmic multiply-adds of the region kernels as run here (symmetric
+// products counted once), per launch, from the realised region sizes; and the
+// reference algorithm's canonical count for the same tree:
+//   prior, level m:     r^3 [m(m-1)/2 + m/2 + m/2 + 1/6]
+//   posterior, level m: r^3 [1/3 + m/2 + m/2 + m(m-1)/2] + r^2 (1/2 + m)
+//   finest region (n observations, L = M-1): r^2 n L(L-1)/2 + L r^2 n/2 + L r n^2/2
+//     + n^3/6 + n^2/2 + L n^2 r/2 + L r n + L r^2 n/2 + L(L-1)/2 r^2 n
+// Factored posterior step of a region with n rows at level m:
+//   r^2 n/2 + r n^2/2 + n^3/6 + n^2/2 + m r n^2/2.
+void make_plan(mra_ctx* c, const HostTree& h) {
+    const int J = c->J, M = c->M;
+    const double R = c->r, Lv = M - 1;
+    double fields = 0;
+    for (int f = 0; f < 3; ++f) fields += (double)c->nb[f];
+    c->plan.clear();
+    c->plan.push_back({MRA_KERNEL_FIELDS, -1, (double)(c->n_int * c->r + c->n_obs + c->n_pred) * (fields * 12 + 8)});
+    double ref = 0;
+    for (int m = 0; m <= M - 2; ++m) {
+        double cnt = std::pow((double)J, m), mm = m;
+        double f = cnt * R * R * R * (mm * (mm - 1) / 2 + mm / 2 + mm / 2 + 1.0 / 6);
+        c->plan.push_back({MRA_KERNEL_PRIOR_LEVEL, m, 2 * f});
+        ref += f + cnt * (R * R * R * (1.0 / 3 + mm / 2 + mm / 2 + mm * (mm - 1) / 2) + R * R * (0.5 + mm));
+    }
+    auto dense_post = [&](double mm) {
+        return R * R * R * (1.0 / 3 + mm / 2 + mm / 2 + mm * (mm - 1) / 2) + R * R * (0.5 + mm);
+    };
+    auto fact_post = [&](double n, double mm) {
+        return R * R * n / 2 + R * n * n / 2 + n * n * n / 6 + n * n / 2 + mm * R * n * n / 2;
+    };
+    auto agg = [&](double n, double mm) { return (mm + 1) * (mm + 2) / 2 * R * R * n + (mm + 1) * R * n; };
+    // finest groups (+ level M-2 posterior)
+    double fin = 0;
+    const long s2 = level_start(J, M - 2), cnt2 = level_count(J, M - 2);
+    for (long q = 0; q < cnt2; ++q) {
+        double np = (double)(h.sub_hi[s2 + q] - h.sub_lo[s2 + q]);
+        fin += R * R * np * Lv * (Lv - 1) / 2 + Lv * R * R * np / 2;
+        for (long k = h.child_lo[q]; k < h.child_hi[q]; ++k) {
+            double n = (double)h.nfin[k];
+            if (n == 0) continue;
+            fin += Lv * R * n * n / 2 + n * n * n / 6 + n * n / 2 + Lv * n * n * R / 2;
+            ref += R * R * n * Lv * (Lv - 1) / 2 + Lv * R * R * n / 2 + Lv * R * n * n / 2 + n * n * n / 6 + n * n / 2 +
+                   Lv * n * n * R / 2 + Lv * R * n + Lv * R * R * n / 2 + Lv * (Lv - 1) / 2 * R * R * n;
+        }
+        fin += h.factored[s2 + q] ? fact_post(np, M - 2) : agg(np, M - 2) + dense_post(M - 2);
+    }
+    c->plan.push_back({MRA_KERNEL_FINEST, M - 1, 2 * fin});
+    const bool split = c->precision == MRA_PRECISION_MIXED;
+    if (split) {
+        // the posterior runs in FP64: FP32 prior factors and B^ are widened first,
+        // and the level M-2 posterior moves out of the finest-group kernel
+        c->plan.push_back({MRA_KERNEL_CONVERT, -1, 0.0});
+        double f2 = 0;
+        for (long q = 0; q < cnt2; ++q) {
+            double np = (double)(h.sub_hi[s2 + q] - h.sub_lo[s2 + q]);
+            f2 += h.factored[s2 + q] ? fact_post(np, M - 2) : agg(np, M - 2) + dense_post(M - 2);
+        }
+        fin -= f2;
+        c->plan.back().flop = 0;
+        c->plan[c->plan.size() - 2].flop = 2 * fin;
+        c->plan.push_back({MRA_KERNEL_POSTERIOR_LEVEL, M - 2, 2 * f2});
+    }
+    for (int m = M - 3; m >= 0; --m) {
+        const long s0 = level_start(J, m), cnt = level_count(J, m);
+        double f = 0;
+        for (long q = 0; q < cnt; ++q) {
+            const long i = s0 + q;
+            double n = (double)(h.sub_hi[i] - h.sub_lo[i]);
+            if (h.factored[i]) {
+                f += fact_post(n, m);
+            } else {
+                for (int cc = 1; cc <= J; ++cc) {
+                    long ch = i * J + cc;
+                    if (h.factored[ch]) f += agg((double)(h.sub_hi[ch] - h.sub_lo[ch]), m);
+                }
+                f += dense_post(m);
+            }
+        }
+        c->plan.push_back({MRA_KERNEL_POSTERIOR_LEVEL, m, 2 * f});
+    }
+    c->plan.push_back({MRA_KERNEL_REDUCE, -1, (double)c->n_int});
+    c->flop_loglik = 0;
+    for (auto& l : c->plan) c->flop_loglik += l.flop;
+    c->flop_reference = 2 * ref;
+}
+
 cudaError_t record(cudaEvent_t e, cudaStream_t st, bool capturing) {
     return capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
 }
 
+// Issues one evaluation on the context's stream: every launch of the plan
+// (plus prediction) bracketed by its own pair of timing events.  The events are
+// recorded as external nodes so that they still time each launch when the
+// sequence is replayed from a captured CUDA graph.
+// FP64 path: every stage on the double tree.  Mixed path: fields, prior and
+// finest level on the FP32 tree, conversion, posterior and reduction on the
+// FP64 tree, prediction on the FP32 tree with the widened-back posterior factors.
 mra_status run_eval(mra_ctx* c, bool predict) {
     cudaStream_t st = c->stream;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CU(cudaStreamIsCapturing(st, &cap));
     const bool capturing = cap == cudaStreamCaptureStatusActive;
-    CU(cudaMemsetAsync(c->t.queue, 0, 4 * sizeof(int), st));
-    CU(cudaMemsetAsync(c->t.err, 0, 4 * sizeof(int), st));
+    const bool mixed = c->precision == MRA_PRECISION_MIXED;
+    DevTree<double>& td = c->td;
+    DevTree<float>& tf = c->tf32;
+    CU(cudaMemsetAsync(td.queue, 0, 4 * sizeof(int), st));
+    CU(cudaMemsetAsync(td.err, 0, 4 * sizeof(int), st));
     const long np_all = c->n_int * c->r + c->n_obs + c->n_pred;
+    const long rr = (long)c->r * c->r;
     int i = 0;
     for (const auto& l : c->plan) {
         CU(record(c->tev[2 * i], st, capturing));
         switch (l.kind) {
             case MRA_KERNEL_FIELDS:
-                launch_fields(c->geom, c->fp, c->t.pts.c0, c->t.pts.c1, c->t.pts.c2, np_all,
-                              const_cast<double*>(c->t.pts.s2), const_cast<double*>(c->t.pts.beta),
-                              const_cast<double*>(c->t.pts.t2), st);
+                launch_fields(c->geom, c->fp, td.pts.c0, td.pts.c1, td.pts.c2, np_all, const_cast<double*>(td.pts.s2),
+                              const_cast<double*>(td.pts.beta), const_cast<double*>(td.pts.t2), st);
                 break;
-            case MRA_KERNEL_PRIOR_LEVEL: launch_prior_level(c->geom, c->t, l.level, c->grid, st); break;
-            case MRA_KERNEL_FINEST: launch_finest(c->geom, c->t, c->grid, predict, st); break;
+            case MRA_KERNEL_PRIOR_LEVEL:
+                if (mixed) launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
+                else launch_prior_level<double>(c->geom, td, l.level, c->grid, st);
+                break;
+            case MRA_KERNEL_FINEST:
+                if (mixed) launch_finest_group<float>(c->geom, tf, c->grid, predict, st);
+                else launch_finest_group<double>(c->geom, td, c->grid, predict, st);
+                break;
+            case MRA_KERNEL_CONVERT:
+                launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
+                launch_convert<float, double>(tf.Bhat, td.Bhat, c->n_obs * (long)c->L * c->r, st);
+                break;
             case MRA_KERNEL_POSTERIOR_LEVEL:
-                launch_posterior_level(c->geom, c->t, l.level, c->grid, predict, st);
+                launch_posterior_level<double>(c->geom, td, l.level, c->grid, predict, st);
                 break;
-            case MRA_KERNEL_REDUCE: launch_reduce(c->t, c->d_result, st); break;
+            case MRA_KERNEL_REDUCE: launch_reduce<double>(td, c->d_result, st); break;
         }
         CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
     }
     if (predict) {
         CU(record(c->tev[2 * i], st, capturing));
-        launch_predict(c->geom, c->t, c->grid, st);
+        if (mixed) {
+            launch_convert<double, float>(td.Lpost, tf.Lpost, c->n_int * rr, st);
+            launch_convert<double, float>(td.G, tf.G, c->u_total, st);
+            launch_predict<float>(c->geom, tf, c->grid, st);
+        } else {
+            launch_predict<double>(c->geom, td, c->grid, st);
+        }
         CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
     }
@@ -222,11 +300,13 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     return MRA_OK;
 }
 
-mra_status finish_eval(mra_ctx* c, bool predict) {
+int* err_ptr(mra_ctx* c) { return c->td.err; }
+
+mra_status finish_eval(mra_ctx* c) {
     CU(cudaStreamSynchronize(c->stream));
     int err[4];
     double d;
-    CU(cudaMemcpy(err, c->t.err, sizeof(err), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(err, err_ptr(c), sizeof(err), cudaMemcpyDeviceToHost));
     CU(cudaMemcpy(&d, c->d_result, sizeof(double), cudaMemcpyDeviceToHost));
     mra_stats& s = c->stats;
     s.ms_fields = s.ms_prior = s.ms_finest = s.ms_posterior = s.ms_predict = s.ms_total = 0;
@@ -234,10 +314,11 @@ mra_status finish_eval(mra_ctx* c, bool predict) {
     for (int i = 0; i < c->n_timed; ++i) {
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, c->tev[2 * i], c->tev[2 * i + 1]));
-        int kind = i < (int)c->plan.size() ? c->plan[i].kind : MRA_KERNEL_PREDICT;
+        const bool in_plan = i < (int)c->plan.size();
+        int kind = in_plan ? c->plan[i].kind : MRA_KERNEL_PREDICT;
         s.timed_kind[i] = kind;
-        s.timed_level[i] = i < (int)c->plan.size() ? c->plan[i].level : -1;
-        s.timed_flop[i] = i < (int)c->plan.size() ? c->plan[i].flop : c->flop_predict_launch;
+        s.timed_level[i] = in_plan ? c->plan[i].level : -1;
+        s.timed_flop[i] = in_plan ? c->plan[i].flop : c->flop_predict_launch;
         s.timed_ms[i] = ms;
         s.ms_total += ms;
         if (kind == MRA_KERNEL_FIELDS) s.ms_fields += ms;
@@ -249,6 +330,7 @@ mra_status finish_eval(mra_ctx* c, bool predict) {
     s.d = d;
     s.loglik = -0.5 * (d + (double)c->n_obs * std::log(2 * 3.14159265359));
     s.flop_last = c->flop_loglik;
+    s.flop_reference = c->flop_reference;
     s.bytes_device = c->bytes;
     s.kernel_launches = c->last_launches;
     s.bad_region = -1;
@@ -258,7 +340,97 @@ mra_status finish_eval(mra_ctx* c, bool predict) {
         std::snprintf(buf, sizeof(buf), "Cholesky pivot not positive in region %lld", (long long)s.bad_region);
         return fail(MRA_ERR_NOT_SPD, buf);
     }
-    (void)predict;
+    return MRA_OK;
+}
+
+// Allocates the typed buffers of one precision and fills its DevTree.
+// Shared FP64 vectors and bookkeeping used by both trees.
+struct Shared {
+    double *yt, *ldprior, *vpost, *dpost, *dfin, *mean, *var;
+    int *queue, *err;
+    int8_t* factored;
+};
+
+template <typename T>
+mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointSet& pts, const double* y,
+                      int64_t* const* idx, int64_t u_total, const Shared& sh, bool prior_part, bool post_part,
+                      bool pred_part) {
+    const int J = c->J, M = c->M, r = c->r, L = c->L;
+    const long rr = (long)r * r;
+    cudaError_t ce = cudaSuccess;
+    t.J = J; t.M = M; t.r = r; t.L = L; t.tf = c->tf;
+    t.n_int = c->n_int; t.n_fin = c->n_fin; t.n_obs = c->n_obs; t.n_pred = c->n_pred;
+    t.obs0 = c->n_int * r;
+    t.pred0 = c->n_int * r + c->n_obs;
+    t.pts = pts;
+    t.y = y;
+    t.obs_off = idx[0]; t.pred_off = idx[1]; t.fin_anc = idx[2]; t.fin_order = idx[3]; t.lsig_off = idx[4];
+    t.pc_off = idx[5]; t.child_lo = idx[6]; t.child_hi = idx[7]; t.par_order = idx[8]; t.sub_lo = idx[9];
+    t.sub_hi = idx[10];
+    // sizes of the level-parity buffers
+    size_t aout_sz[2] = {1, 1}, wout_sz[2] = {1, 1}, F_sz[2] = {1, 1}, f_sz[2] = {1, 1};
+    for (int m = 1; m <= M - 2; ++m) {
+        const long s0 = level_start(J, m), cnt = level_count(J, m);
+        bool any_dense = false, any_fact = false;
+        for (long q = 0; q < cnt; ++q) (h.factored[s0 + q] ? any_fact : any_dense) = true;
+        if (any_dense) {
+            aout_sz[m & 1] = std::max(aout_sz[m & 1], (size_t)(cnt * n_slices(m) * rr));
+            wout_sz[m & 1] = std::max(wout_sz[m & 1], (size_t)(cnt * m * r));
+        }
+        if (any_fact) {
+            F_sz[m & 1] = std::max(F_sz[m & 1], (size_t)(c->n_obs * (long)m * r));
+            f_sz[m & 1] = std::max(f_sz[m & 1], (size_t)c->n_obs);
+        }
+    }
+    t.ws_stride = post_part ? std::max((long)r * c->tf + (long)c->tf * c->tf, n_slices(M - 1) * rr + (long)(M - 2) * rr) + 64
+                            : 64;
+    t.wsd_stride = post_part ? (long)(M - 1) * r + c->tf + 64 : 64;
+    if (!post_part) {
+        for (int p = 0; p < 2; ++p) aout_sz[p] = wout_sz[p] = F_sz[p] = f_sz[p] = 1;
+    }
+    const bool need_lpost_g = post_part || pred_part;
+#define TALLOC(ptr, TYPE, n)                                                                          \
+    do {                                                                                              \
+        ptr = c->alloc<TYPE>((size_t)(n), &ce);                                                       \
+        if (ce) return fail(MRA_ERR_OOM, std::string("device allocation failed: ") + #ptr);           \
+    } while (0)
+    TALLOC(t.Lprior, T, c->n_int * rr);
+    TALLOC(t.Bhat, T, c->n_obs * (long)L * r);
+    TALLOC(t.U, T, prior_part ? u_total : 1);
+    TALLOC(t.Ufin, T, prior_part ? c->n_obs * (long)L * r : 1);
+    TALLOC(t.Lsig, T, prior_part ? h.lsig_off[c->n_fin] : 1);
+    TALLOC(t.Lpost, T, need_lpost_g ? c->n_int * rr : 1);
+    TALLOC(t.G, T, need_lpost_g && c->have_pred ? u_total : 1);
+    for (int p = 0; p < 2; ++p) {
+        TALLOC(t.aout[p], T, aout_sz[p]);
+        TALLOC(t.wout[p], double, wout_sz[p]);
+        TALLOC(t.Fbuf[p], T, F_sz[p]);
+        TALLOC(t.fbuf[p], double, f_sz[p]);
+    }
+    TALLOC(t.ws, T, (long)c->grid * t.ws_stride);
+    TALLOC(t.wsd, double, (long)c->grid * t.wsd_stride);
+    TALLOC(t.P, T, pred_part ? c->n_pred * (long)L * r : 1);
+    TALLOC(t.Bt, T, pred_part ? c->n_pred * (long)L * r : 1);
+    TALLOC(t.Pc, T, pred_part ? h.pc_off[c->n_fin] : 1);
+#undef TALLOC
+    t.yt = sh.yt;
+    t.ldprior = sh.ldprior;
+    t.vpost = sh.vpost;
+    t.dpost = sh.dpost;
+    t.dfin = sh.dfin;
+    t.mean = sh.mean;
+    t.var = sh.var;
+    t.queue = sh.queue;
+    t.err = sh.err;
+    t.factored = sh.factored;
+    t.fuse_post = (prior_part && post_part) ? 1 : 0;
+    int64_t uo = 0;
+    for (int m = 0; m < kMaxLevels; ++m) t.u_off[m] = 0;
+    for (int m = 0; m <= M - 2; ++m) {
+        t.u_off[m] = uo;
+        uo += level_count(J, m) * (int64_t)m * r * r;
+    }
+    (void)u_total;
     return MRA_OK;
 }
 
@@ -273,22 +445,6 @@ mra_status mra_set_device(int32_t device) {
     if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
         return fail(MRA_ERR_NO_DEVICE, "no such CUDA device");
     CU(cudaSetDevice(device));
-    return MRA_OK;
-}
-
-mra_status mra_timer_start(mra_ctx* c) {
-    if (!c) return fail(MRA_ERR_ARG, "NULL context");
-    CU(cudaEventRecord(c->ev[6], c->stream));
-    return MRA_OK;
-}
-
-mra_status mra_timer_stop(mra_ctx* c, double* ms) {
-    if (!c || !ms) return fail(MRA_ERR_ARG, "NULL argument");
-    CU(cudaEventRecord(c->ev[7], c->stream));
-    CU(cudaEventSynchronize(c->ev[7]));
-    float f = 0;
-    CU(cudaEventElapsedTime(&f, c->ev[6], c->ev[7]));
-    *ms = f;
     return MRA_OK;
 }
 
@@ -309,33 +465,40 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     const long n_fin = (long)s->n_finest;
     if (n_fin < 1 || !s->finest_parent || !s->knots || !s->obs_offset)
         return fail(MRA_ERR_ARG, "structure arrays are NULL or empty");
-    const long n_obs = (long)s->obs_offset[n_fin];
     if (s->obs_offset[0] != 0) return fail(MRA_ERR_ARG, "obs_offset[0] must be 0");
+    const long n_obs = (long)s->obs_offset[n_fin];
     if (n_obs > 0 && (!s->obs || !s->obs_value)) return fail(MRA_ERR_ARG, "observation arrays are NULL");
     const long lvl2 = level_start(J, M - 2), cnt2 = level_count(J, M - 2);
-    std::vector<int64_t> nfin(n_fin), child_lo(cnt2, -1), child_hi(cnt2, -1);
+    HostTree h;
+    h.nfin.assign(n_fin, 0);
+    h.npred.assign(n_fin, 0);
+    h.child_lo.assign(cnt2, -1);
+    h.child_hi.assign(cnt2, -1);
+    long prev_parent = -1;
     for (long k = 0; k < n_fin; ++k) {
         if (s->obs_offset[k + 1] < s->obs_offset[k]) return fail(MRA_ERR_ARG, "obs_offset must be non-decreasing");
-        nfin[k] = (int64_t)(s->obs_offset[k + 1] - s->obs_offset[k]);
+        h.nfin[k] = (int64_t)(s->obs_offset[k + 1] - s->obs_offset[k]);
         long p = (long)s->finest_parent[k];
         if (p < lvl2 || p >= lvl2 + cnt2) return fail(MRA_ERR_ARG, "finest_parent must be a level M-2 region");
+        if (p < prev_parent)
+            return fail(MRA_ERR_ARG, "finest regions must be ordered by parent (children of a region contiguous)");
+        prev_parent = p;
         long q = p - lvl2;
-        if (child_lo[q] < 0) child_lo[q] = k;
-        else if (child_hi[q] != k) return fail(MRA_ERR_ARG, "finest children of a region must be contiguous");
-        child_hi[q] = k + 1;
+        if (h.child_lo[q] < 0) h.child_lo[q] = k;
+        h.child_hi[q] = k + 1;
     }
     for (long q = 0; q < cnt2; ++q)
-        if (child_lo[q] < 0) child_lo[q] = child_hi[q] = 0;
+        if (h.child_lo[q] < 0) h.child_lo[q] = h.child_hi[q] = 0;
     long n_pred = 0;
-    bool have_pred = s->pred_offset != nullptr;
-    std::vector<int64_t> npred(n_fin, 0);
-    if (have_pred) {
+    const bool have_pred_arr = s->pred_offset != nullptr;
+    if (have_pred_arr) {
         if (s->pred_offset[0] != 0) return fail(MRA_ERR_ARG, "pred_offset[0] must be 0");
         n_pred = (long)s->pred_offset[n_fin];
         if (n_pred > 0 && !s->pred) return fail(MRA_ERR_ARG, "prediction coordinates are NULL");
         for (long k = 0; k < n_fin; ++k) {
-            if (s->pred_offset[k + 1] < s->pred_offset[k]) return fail(MRA_ERR_ARG, "pred_offset must be non-decreasing");
-            npred[k] = (int64_t)(s->pred_offset[k + 1] - s->pred_offset[k]);
+            if (s->pred_offset[k + 1] < s->pred_offset[k])
+                return fail(MRA_ERR_ARG, "pred_offset must be non-decreasing");
+            h.npred[k] = (int64_t)(s->pred_offset[k + 1] - s->pred_offset[k]);
         }
     }
 
@@ -357,7 +520,9 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     c->grid = 2 * c->sms;
     c->J = J; c->M = M; c->r = r; c->L = L;
     c->n_int = n_int; c->n_fin = n_fin; c->n_obs = n_obs; c->n_pred = n_pred;
-    c->have_pred = have_pred && n_pred > 0;
+    c->have_pred = have_pred_arr && n_pred > 0;
+    c->tf = 2 * r;
+    if (const char* e = std::getenv("MRA_FACTORED_MAX")) c->tf = std::max(0, std::atoi(e));
     c->geom = make_geom(m);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(MRA_ERR_CUDA, "stream creation failed"));
@@ -367,136 +532,146 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "event creation failed"));
 
     // host-side tables
-    std::vector<int64_t> obs_off(n_fin + 1), pred_off(n_fin + 1, 0), fin_anc(n_fin * L), lsig_off(n_fin + 1),
-        pc_off(n_fin + 1), fin_order(n_fin);
-    lsig_off[0] = pc_off[0] = 0;
+    h.obs_off.assign(n_fin + 1, 0);
+    h.pred_off.assign(n_fin + 1, 0);
+    h.fin_anc.assign(n_fin * L, 0);
+    h.lsig_off.assign(n_fin + 1, 0);
+    h.pc_off.assign(n_fin + 1, 0);
+    h.fin_order.assign(n_fin, 0);
     for (long k = 0; k <= n_fin; ++k) {
-        obs_off[k] = (int64_t)s->obs_offset[k];
-        if (have_pred) pred_off[k] = (int64_t)s->pred_offset[k];
+        h.obs_off[k] = (int64_t)s->obs_offset[k];
+        if (have_pred_arr) h.pred_off[k] = (int64_t)s->pred_offset[k];
     }
     for (long k = 0; k < n_fin; ++k) {
         long a = (long)s->finest_parent[k];
-        fin_anc[k * L + L - 1] = a;
+        h.fin_anc[k * L + L - 1] = a;
         for (int j = L - 2; j >= 0; --j) {
             a = (a - 1) / J;
-            fin_anc[k * L + j] = a;
+            h.fin_anc[k * L + j] = a;
         }
-        lsig_off[k + 1] = lsig_off[k] + nfin[k] * nfin[k];
-        pc_off[k + 1] = pc_off[k] + nfin[k] * npred[k];
-        fin_order[k] = k;
+        h.lsig_off[k + 1] = h.lsig_off[k] + h.nfin[k] * h.nfin[k];
+        h.pc_off[k + 1] = h.pc_off[k] + h.nfin[k] * h.npred[k];
+        h.fin_order[k] = k;
     }
-    std::stable_sort(fin_order.begin(), fin_order.end(),
-                     [&](int64_t a, int64_t b) { return nfin[a] + npred[a] > nfin[b] + npred[b]; });
+    std::stable_sort(h.fin_order.begin(), h.fin_order.end(), [&](int64_t a, int64_t b) {
+        return h.npred[a] * (h.nfin[a] + 1) > h.npred[b] * (h.nfin[b] + 1);
+    });
+    // subtree observation ranges and the factored / dense decision per interior region
+    h.sub_lo.assign(n_int, 0);
+    h.sub_hi.assign(n_int, 0);
+    h.factored.assign(n_int, 0);
+    for (long q = 0; q < cnt2; ++q) {
+        h.sub_lo[lvl2 + q] = h.obs_off[h.child_lo[q]];
+        h.sub_hi[lvl2 + q] = h.child_hi[q] > h.child_lo[q] ? h.obs_off[h.child_hi[q]] : h.sub_lo[lvl2 + q];
+    }
+    for (int mm = M - 3; mm >= 0; --mm) {
+        const long s0 = level_start(J, mm), cnt = level_count(J, mm);
+        for (long q = 0; q < cnt; ++q) {
+            long i = s0 + q, lo = -1, hi = -1;
+            for (int cc = 1; cc <= J; ++cc) {
+                long ch = i * J + cc;
+                if (h.sub_hi[ch] > h.sub_lo[ch]) {
+                    if (lo < 0) lo = h.sub_lo[ch];
+                    hi = h.sub_hi[ch];
+                }
+            }
+            h.sub_lo[i] = lo < 0 ? 0 : lo;
+            h.sub_hi[i] = lo < 0 ? 0 : hi;
+        }
+    }
+    for (long i = 0; i < n_int; ++i) h.factored[i] = (h.sub_hi[i] - h.sub_lo[i]) <= c->tf ? 1 : 0;
+    h.par_order.assign(cnt2, 0);
+    for (long q = 0; q < cnt2; ++q) h.par_order[q] = q;
+    std::stable_sort(h.par_order.begin(), h.par_order.end(), [&](int64_t a, int64_t b) {
+        double na = (double)(h.sub_hi[lvl2 + a] - h.sub_lo[lvl2 + a]);
+        double nb = (double)(h.sub_hi[lvl2 + b] - h.sub_lo[lvl2 + b]);
+        return na * (na + 64.0 * L) > nb * (nb + 64.0 * L);
+    });
     int64_t u_total = 0;
-    for (int mm = 0; mm < kMaxLevels; ++mm) c->t.u_off[mm] = 0;
-    for (int mm = 0; mm <= M - 2; ++mm) {
-        c->t.u_off[mm] = u_total;
-        u_total += level_count(J, mm) * (int64_t)mm * r * r;
-    }
-    // posterior outputs: ping-pong by level parity
-    size_t aout_sz[2] = {16, 16}, wout_sz[2] = {16, 16};
-    for (int mm = 1; mm <= M - 2; ++mm) {
-        aout_sz[mm & 1] = std::max(aout_sz[mm & 1], (size_t)(level_count(J, mm) * n_slices(mm) * r * r));
-        wout_sz[mm & 1] = std::max(wout_sz[mm & 1], (size_t)(level_count(J, mm) * mm * r));
-    }
-    const long rr = (long)r * r;
-    c->t.ws_stride = n_slices(M - 1) * rr + (long)(M - 1) * r + (long)(M - 2 > 0 ? M - 2 : 0) * rr;
+    for (int mm = 0; mm <= M - 2; ++mm) u_total += level_count(J, mm) * (int64_t)mm * r * r;
 
+    // shared device arrays: coordinates, fields, observations, index tables
     cudaError_t ce = cudaSuccess;
     const long np_all = n_int * r + n_obs + n_pred;
     double* pc[3];
-    for (int d = 0; d < 3; ++d) {
-        pc[d] = c->alloc<double>(np_all, &ce);
-        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed"));
-    }
     double* fields[3];
     for (int d = 0; d < 3; ++d) {
+        pc[d] = c->alloc<double>(np_all, &ce);
+        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: coordinates"));
         fields[d] = c->alloc<double>(np_all, &ce);
-        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed"));
+        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: fields"));
     }
-    DevTree& t = c->t;
-    t.J = J; t.M = M; t.r = r; t.L = L;
-    t.n_int = n_int; t.n_fin = n_fin; t.n_obs = n_obs; t.n_pred = n_pred;
-    t.obs0 = n_int * r;
-    t.pred0 = n_int * r + n_obs;
-    t.pts = PointSet{pc[0], pc[1], pc[2], fields[0], fields[1], fields[2]};
-#define ALLOC(ptr, T, n)                                                   \
-    do {                                                                   \
-        ptr = c->alloc<T>((size_t)(n), &ce);                               \
-        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: " #ptr)); \
-    } while (0)
-    double* y;
-    ALLOC(y, double, n_obs);
-    t.y = y;
-    int64_t *d_obs_off, *d_pred_off, *d_fin_anc, *d_fin_order, *d_lsig_off, *d_pc_off, *d_clo, *d_chi;
-    ALLOC(d_obs_off, int64_t, n_fin + 1);
-    ALLOC(d_pred_off, int64_t, n_fin + 1);
-    ALLOC(d_fin_anc, int64_t, n_fin * L);
-    ALLOC(d_fin_order, int64_t, n_fin);
-    ALLOC(d_lsig_off, int64_t, n_fin + 1);
-    ALLOC(d_pc_off, int64_t, n_fin + 1);
-    ALLOC(d_clo, int64_t, cnt2);
-    ALLOC(d_chi, int64_t, cnt2);
-    t.obs_off = d_obs_off; t.pred_off = d_pred_off; t.fin_anc = d_fin_anc; t.fin_order = d_fin_order;
-    t.lsig_off = d_lsig_off; t.pc_off = d_pc_off; t.child_lo = d_clo; t.child_hi = d_chi;
-    ALLOC(t.Lprior, double, n_int * rr);
-    ALLOC(t.Lpost, double, n_int * rr);
-    ALLOC(t.U, double, u_total);
-    ALLOC(t.Ufin, double, n_obs * (long)L * r);
-    ALLOC(t.Bhat, double, n_obs * (long)L * r);
-    ALLOC(t.yt, double, n_obs);
-    ALLOC(t.Lsig, double, lsig_off[n_fin]);
-    ALLOC(t.dfin, double, n_fin);
-    ALLOC(t.vpost, double, n_int * r);
-    ALLOC(t.G, double, c->have_pred ? u_total : 1);
-    ALLOC(t.dpost, double, n_int);
-    ALLOC(t.aout[0], double, aout_sz[0]);
-    ALLOC(t.aout[1], double, aout_sz[1]);
-    ALLOC(t.wout[0], double, wout_sz[0]);
-    ALLOC(t.wout[1], double, wout_sz[1]);
-    ALLOC(t.ws, double, (long)c->grid * t.ws_stride);
-    ALLOC(t.P, double, n_pred * (long)L * r);
-    ALLOC(t.Bt, double, n_pred * (long)L * r);
-    ALLOC(t.Pc, double, pc_off[n_fin]);
-    ALLOC(t.mean, double, n_pred);
-    ALLOC(t.var, double, n_pred);
-    ALLOC(t.queue, int, 4);
-    ALLOC(t.err, int, 4);
-    ALLOC(c->d_theta, double, 16);
-    ALLOC(c->d_result, double, 4);
+    double* y = c->alloc<double>(n_obs, &ce);
+    if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: y"));
+    const std::vector<int64_t>* tabs[11] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.fin_order, &h.lsig_off,
+                                            &h.pc_off, &h.child_lo, &h.child_hi, &h.par_order, &h.sub_lo, &h.sub_hi};
+    int64_t* idx[11];
+    for (int q = 0; q < 11; ++q) {
+        idx[q] = c->alloc<int64_t>(tabs[q]->size(), &ce);
+        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: index tables"));
+        mra_status u = upload(idx[q], tabs[q]->data(), tabs[q]->size() * sizeof(int64_t), c->stream);
+        if (u) return bail(u);
+    }
+    c->d_theta = c->alloc<double>(16, &ce);
+    if (!ce) c->d_result = c->alloc<double>(4, &ce);
+    if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed"));
     for (int f = 0; f < 3; ++f) {
         c->nb[f] = m->nonstationary ? (long)m->field[f].n_basis : 0;
-        double* centers;
-        ALLOC(centers, double, 3 * c->nb[f]);
-        ALLOC(c->d_weights[f], double, c->nb[f]);
+        double* centers = c->alloc<double>(3 * c->nb[f], &ce);
+        if (!ce) c->d_weights[f] = c->alloc<double>(c->nb[f], &ce);
+        if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: basis"));
         c->model_weights[f].assign(m->nonstationary && c->nb[f] ? m->field[f].weights : nullptr,
                                    m->nonstationary && c->nb[f] ? m->field[f].weights + c->nb[f] : nullptr);
         c->model_intercept[f] = m->nonstationary ? m->field[f].intercept : 0.0;
         if (c->nb[f]) {
             mra_status u = upload(centers, m->field[f].centers, 3 * c->nb[f] * sizeof(double), c->stream);
-            if (u) return bail(u);
-            u = upload(c->d_weights[f], m->field[f].weights, c->nb[f] * sizeof(double), c->stream);
+            if (!u) u = upload(c->d_weights[f], m->field[f].weights, c->nb[f] * sizeof(double), c->stream);
             if (u) return bail(u);
         }
         c->fp.nb[f] = c->nb[f];
         c->fp.centers[f] = centers;
         c->fp.weights[f] = c->d_weights[f];
     }
-#undef ALLOC
-    make_plan(c, nfin);
+    c->fp.basis = m->basis;
+    c->fp.basis_len = m->basis_len;
+    c->fp.theta = c->d_theta;
+    PointSet pts{pc[0], pc[1], pc[2], fields[0], fields[1], fields[2]};
+    Shared sh{};
+    sh.yt = c->alloc<double>(n_obs, &ce);
+    if (!ce) sh.ldprior = c->alloc<double>(n_int, &ce);
+    if (!ce) sh.vpost = c->alloc<double>(n_int * r, &ce);
+    if (!ce) sh.dpost = c->alloc<double>(n_int, &ce);
+    if (!ce) sh.dfin = c->alloc<double>(cnt2, &ce);
+    if (!ce) sh.mean = c->alloc<double>(n_pred, &ce);
+    if (!ce) sh.var = c->alloc<double>(n_pred, &ce);
+    if (!ce) sh.queue = c->alloc<int>(4, &ce);
+    if (!ce) sh.err = c->alloc<int>(4, &ce);
+    if (!ce) sh.factored = c->alloc<int8_t>(n_int, &ce);
+    if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: shared vectors"));
+    {
+        mra_status u = upload(sh.factored, h.factored.data(), n_int * sizeof(int8_t), c->stream);
+        if (u) return bail(u);
+        CU(cudaMemsetAsync(sh.dpost, 0, n_int * sizeof(double), c->stream));
+    }
+    c->u_total = u_total;
+    mra_status st;
+    if (precision == MRA_PRECISION_MIXED) {
+        st = setup_tree<float>(c, c->tf32, h, pts, y, idx, u_total, sh, true, false, c->have_pred);
+        if (!st) st = setup_tree<double>(c, c->td, h, pts, y, idx, u_total, sh, false, true, false);
+    } else {
+        st = setup_tree<double>(c, c->td, h, pts, y, idx, u_total, sh, true, true, c->have_pred);
+    }
+    if (st) return bail(st);
+    make_plan(c, h);
     {
         double R = r, fl = 0;
         for (long k = 0; k < n_fin; ++k) {
-            double np = (double)npred[k], n = (double)nfin[k];
+            double np = (double)h.npred[k], n = (double)h.nfin[k];
             fl += np * (L * R * R * (L - 1) / 2 + L * R * R / 2 + n * L * R + n * n / 2 + L * R * n + L * R * R / 2 +
                         L * (L - 1) / 2 * R * R);
         }
         c->flop_predict_launch = 2 * fl;
     }
-    c->fp.basis = m->basis;
-    c->fp.basis_len = m->basis_len;
-    c->fp.theta = c->d_theta;
-
     // upload the structure (coordinates: knots | obs | preds per coordinate)
     for (int d = 0; d < 3; ++d) {
         mra_status u = upload(pc[d], s->knots + (size_t)d * n_int * r, n_int * r * sizeof(double), c->stream);
@@ -505,29 +680,14 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
             u = upload(pc[d] + n_int * r + n_obs, s->pred + (size_t)d * n_pred, n_pred * sizeof(double), c->stream);
         if (u) return bail(u);
     }
-    struct {
-        void* dst;
-        const void* src;
-        size_t bytes;
-    } ups[] = {
-        {y, s->obs_value, n_obs * sizeof(double)},
-        {d_obs_off, obs_off.data(), (n_fin + 1) * sizeof(int64_t)},
-        {d_pred_off, pred_off.data(), (n_fin + 1) * sizeof(int64_t)},
-        {d_fin_anc, fin_anc.data(), n_fin * L * sizeof(int64_t)},
-        {d_fin_order, fin_order.data(), n_fin * sizeof(int64_t)},
-        {d_lsig_off, lsig_off.data(), (n_fin + 1) * sizeof(int64_t)},
-        {d_pc_off, pc_off.data(), (n_fin + 1) * sizeof(int64_t)},
-        {d_clo, child_lo.data(), cnt2 * sizeof(int64_t)},
-        {d_chi, child_hi.data(), cnt2 * sizeof(int64_t)},
-    };
-    for (auto& u : ups) {
-        mra_status e = upload(u.dst, u.src, u.bytes, c->stream);
-        if (e) return bail(e);
+    {
+        mra_status u = upload(y, s->obs_value, n_obs * sizeof(double), c->stream);
+        if (u) return bail(u);
     }
     double th0[16] = {1, 1, 1, c->model_intercept[0], c->model_intercept[1], c->model_intercept[2], 1, 1, 0};
     {
-        mra_status e = upload(c->d_theta, th0, sizeof(th0), c->stream);
-        if (e) return bail(e);
+        mra_status u = upload(c->d_theta, th0, sizeof(th0), c->stream);
+        if (u) return bail(u);
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "upload failed"));
     *out = c;
@@ -550,6 +710,8 @@ mra_status mra_set_theta(mra_ctx* c, const mra_theta* th) {
     v[6] = th->sill; v[7] = th->range; v[8] = th->nugget;
     if (!c->geom.nonstat && !(v[6] > 0 && v[7] > 0 && v[8] >= 0))
         return fail(MRA_ERR_ARG, "sill and range must be positive, nugget non-negative");
+    for (int f = 3; f < 6; ++f)
+        if (!std::isfinite(v[f])) return fail(MRA_ERR_ARG, "intercepts must be finite");
     CU(cudaMemcpyAsync(c->d_theta, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
     for (int f = 0; f < 3; ++f) {
         if (!c->nb[f]) continue;
@@ -561,7 +723,8 @@ mra_status mra_set_theta(mra_ctx* c, const mra_theta* th) {
 
 mra_status mra_set_obs_values(mra_ctx* c, const double* y) {
     if (!c || (!y && c->n_obs)) return fail(MRA_ERR_ARG, "NULL argument");
-    CU(cudaMemcpyAsync(const_cast<double*>(c->t.y), y, c->n_obs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double* dy = c->td.y;
+    CU(cudaMemcpyAsync(const_cast<double*>(dy), y, c->n_obs * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     return MRA_OK;
 }
 
@@ -574,7 +737,7 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
         mra_status s = run_eval(c, false);
         if (s) return s;
     }
-    mra_status s = finish_eval(c, false);
+    mra_status s = finish_eval(c);
     if (d_out) *d_out = c->stats.d;
     if (ll_out) *ll_out = c->stats.loglik;
     return s;
@@ -585,10 +748,12 @@ mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     if (!c->have_pred) return fail(MRA_ERR_STATE, "the structure has no prediction locations");
     mra_status s = run_eval(c, true);
     if (s) return s;
-    s = finish_eval(c, true);
+    s = finish_eval(c);
     if (s) return s;
-    if (mean) CU(cudaMemcpy(mean, c->t.mean, c->n_pred * sizeof(double), cudaMemcpyDeviceToHost));
-    if (var) CU(cudaMemcpy(var, c->t.var, c->n_pred * sizeof(double), cudaMemcpyDeviceToHost));
+    const double* dm = c->td.mean;
+    const double* dv = c->td.var;
+    if (mean) CU(cudaMemcpy(mean, dm, c->n_pred * sizeof(double), cudaMemcpyDeviceToHost));
+    if (var) CU(cudaMemcpy(var, dv, c->n_pred * sizeof(double), cudaMemcpyDeviceToHost));
     return MRA_OK;
 }
 
@@ -614,30 +779,51 @@ mra_status mra_get_stats(const mra_ctx* c, mra_stats* out) {
     *out = c->stats;
     out->bytes_device = c->bytes;
     out->flop_last = c->flop_loglik;
+    out->flop_reference = c->flop_reference;
+    return MRA_OK;
+}
+
+mra_status mra_timer_start(mra_ctx* c) {
+    if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    CU(cudaEventRecord(c->ev[6], c->stream));
+    return MRA_OK;
+}
+
+mra_status mra_timer_stop(mra_ctx* c, double* ms) {
+    if (!c || !ms) return fail(MRA_ERR_ARG, "NULL argument");
+    CU(cudaEventRecord(c->ev[7], c->stream));
+    CU(cudaEventSynchronize(c->ev[7]));
+    float f = 0;
+    CU(cudaEventElapsedTime(&f, c->ev[6], c->ev[7]));
+    *ms = f;
     return MRA_OK;
 }
 
 mra_status mra_sample_prior(mra_ctx* c, const double* z_int, const double* z_obs, double* y_out) {
     if (!c || !z_int || (!z_obs && c->n_obs) || (!y_out && c->n_obs)) return fail(MRA_ERR_ARG, "NULL argument");
-    // the prior factors come from one evaluation in prediction layout (keeps U_fin, L_Sigma)
+    // the prior factors (U of the finest level, L_Sigma) come from one evaluation
     mra_status s = run_eval(c, false);
     if (s) return s;
-    s = finish_eval(c, false);
+    s = finish_eval(c);
     if (s) return s;
-    double *dz, *dzo, *dy;
+    double *dz = nullptr, *dzo = nullptr, *dy = nullptr;
     size_t nzi = (size_t)c->n_int * c->r;
-    CU(cudaMalloc(&dz, nzi * sizeof(double)));
-    CU(cudaMalloc(&dzo, std::max<size_t>(c->n_obs, 1) * sizeof(double)));
-    CU(cudaMalloc(&dy, std::max<size_t>(c->n_obs, 1) * sizeof(double)));
-    CU(cudaMemcpy(dz, z_int, nzi * sizeof(double), cudaMemcpyHostToDevice));
-    if (c->n_obs) CU(cudaMemcpy(dzo, z_obs, c->n_obs * sizeof(double), cudaMemcpyHostToDevice));
-    launch_sample(c->t, dz, dzo, dy, c->grid, c->stream);
-    CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(c->stream));
-    if (c->n_obs) CU(cudaMemcpy(y_out, dy, c->n_obs * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaError_t e = cudaMalloc(&dz, nzi * sizeof(double));
+    if (!e) e = cudaMalloc(&dzo, std::max<size_t>(c->n_obs, 1) * sizeof(double));
+    if (!e) e = cudaMalloc(&dy, std::max<size_t>(c->n_obs, 1) * sizeof(double));
+    if (!e) e = cudaMemcpy(dz, z_int, nzi * sizeof(double), cudaMemcpyHostToDevice);
+    if (!e && c->n_obs) e = cudaMemcpy(dzo, z_obs, c->n_obs * sizeof(double), cudaMemcpyHostToDevice);
+    if (!e) {
+        if (c->precision == MRA_PRECISION_MIXED) launch_sample<float>(c->tf32, dz, dzo, dy, c->grid, c->stream);
+        else launch_sample<double>(c->td, dz, dzo, dy, c->grid, c->stream);
+        e = cudaGetLastError();
+    }
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    if (!e && c->n_obs) e = cudaMemcpy(y_out, dy, c->n_obs * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(dz);
     cudaFree(dzo);
     cudaFree(dy);
+    if (e) return fail(e == cudaErrorMemoryAllocation ? MRA_ERR_OOM : MRA_ERR_CUDA, cudaGetErrorString(e));
     return MRA_OK;
 }
 

@@ -2,11 +2,17 @@
 //
 //  * covariance entries, following src/evaluate_covariance.cpp:155-313 and the
 //    fields of src/class_nonstationary_covariance.cpp:479-573;
-//  * CTA-cooperative FP64 dense primitives on column-major operands that may
-//    live in global or shared memory: tiled GEMM, blocked left / right
-//    triangular solves and a blocked right-looking Cholesky.  One CTA owns one
-//    region's problem; the region kernels in mra_kernels.cu are sequences of
-//    these calls.
+//  * CTA-cooperative dense primitives on column-major operands that may live
+//    in global or shared memory, templated on the storage type T:
+//      T = double  the plain FP64 path: products on the FP64 tensor pipe
+//                  (mma.sync m8n8k4 f64);
+//      T = float   the mixed path: operands stored in FP32, products on the
+//                  tensor cores as three TF32 products (hi*hi + hi*lo + lo*hi,
+//                  FP32-accurate) with FP32 accumulation.
+//    Diagonal blocks of every Cholesky factorization and triangular solve are
+//    computed in FP64 whatever T is, and log-determinants are accumulated in
+//    FP64.  One CTA owns one region's problem; the region kernels in
+//    mra_kernels.cu are sequences of these calls.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -55,6 +61,14 @@ __device__ __forceinline__ double matern(int nu_x2, double h) {
     return exp(-h);
 }
 
+__device__ __forceinline__ float matern_f(int nu_x2, float h) {
+    if (nu_x2 == 3) {
+        float s = 1.7320508f * h;
+        return (1.0f + s) * expf(-s);
+    }
+    return expf(-h);
+}
+
 // C(s1, s2) with per-point sigma^2 (s) and beta (b): evaluate_covariance.cpp:218-225
 // (nonstationary) and :82 (stationary: s1 = sill, b1 = range).
 __device__ __forceinline__ double cov_entry(const Geom& g, const Pt& p1, double s1, double b1, const Pt& p2,
@@ -66,6 +80,23 @@ __device__ __forceinline__ double cov_entry(const Geom& g, const Pt& p1, double 
     double pre = g.pref_kind == 0 ? x * sqrt(x) : (g.pref_kind == 1 ? x : pow(x, g.pref_exp));
     double c = sqrt(s1 * s2) * pre;
     return c * matern(g.nu_x2, D / sqrt(bms));
+}
+
+// The same entry evaluated in FP32 (the mixed path's covariance evaluation).
+__device__ __forceinline__ float cov_entry_f(const Geom& g, const Pt& p1, float s1, float b1, const Pt& p2, float s2,
+                                             float b2) {
+    float D;
+    if (g.distance == 1) {
+        D = (float)(g.dist_scale * point_distance(g, p1, p2));
+    } else {
+        float dx = (float)(p2.c0 - p1.c0), dy = (float)(p2.c1 - p1.c1), dz = (float)(p2.c2 - p1.c2);
+        D = (float)g.dist_scale * sqrtf(dx * dx + dy * dy + dz * dz);
+    }
+    if (!g.nonstat) return s1 * matern_f(g.nu_x2, D / b1);
+    float bms = (b1 * b1 + b2 * b2) * 0.5f;
+    float x = (b1 * b2) / bms;
+    float pre = g.pref_kind == 0 ? x * sqrtf(x) : (g.pref_kind == 1 ? x : powf(x, (float)g.pref_exp));
+    return sqrtf(s1 * s2) * pre * matern_f(g.nu_x2, D / sqrtf(bms));
 }
 
 // A point set laid out SoA: coordinates c0/c1/c2 and fields s2 (sigma^2),
@@ -82,113 +113,267 @@ struct PointSet {
 
 // out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
 // diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
-__device__ inline void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
-                                double* out, long ld) {
+template <typename T>
+__device__ inline void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self, T* out,
+                                long ld) {
     for (int e = threadIdx.x; e < na * nb; e += blockDim.x) {
         int t = e % na, q = e / na;
         long ia = a0 + t, ib = b0 + q;
-        double v;
+        T v;
         if (self && t == q) {
-            v = P.s2[ia] + P.t2[ia];
+            v = (T)(P.s2[ia] + P.t2[ia]);
+        } else if (sizeof(T) == 8) {
+            v = (T)cov_entry(g, P.pt(ia), P.s2[ia], P.beta[ia], P.pt(ib), P.s2[ib], P.beta[ib]);
         } else {
-            v = cov_entry(g, P.pt(ia), P.s2[ia], P.beta[ia], P.pt(ib), P.s2[ib], P.beta[ib]);
+            v = (T)cov_entry_f(g, P.pt(ia), (float)P.s2[ia], (float)P.beta[ia], P.pt(ib), (float)P.s2[ib],
+                               (float)P.beta[ib]);
         }
         out[t + (long)q * ld] = v;
     }
 }
 
 // ----------------------------------------------------------------------------
-// CTA-cooperative FP64 dense linear algebra (column-major)
+// tensor-pipe fragments
 // ----------------------------------------------------------------------------
-constexpr int TM = 64, TN = 64, TK = 16, NB = 32;
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
 
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// ----------------------------------------------------------------------------
+// CTA-cooperative dense linear algebra (column-major)
+// ----------------------------------------------------------------------------
+constexpr int TM = 64, TN = 64, TK = 16, NB = 16;
+
+template <typename T>
+struct TilePad;
+template <>
+struct TilePad<double> {
+    static constexpr int v = 4;  // row stride 68 doubles: conflict-free m8n8k4 fragment loads
+};
+template <>
+struct TilePad<float> {
+    static constexpr int v = 8;  // row stride 72 floats: conflict-free m16n8k8 fragment loads
+};
+
+template <typename T>
 struct LaSmem {
-    double A[TK][TM + 1];
-    double B[TK][TN + 1];
-    double D[NB][NB + 1];  // staged diagonal block for the triangular kernels
+    T A[TK][TM + TilePad<T>::v];
+    T B[TK][TN + TilePad<T>::v];
+    double D[NB][NB + 1];  // staged diagonal block (always FP64)
     double red[kThreads / 32];
     int flag;
 };
 
-// C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N.
-// beta == 0 never reads C.  Ends with a barrier.
-template <bool TA, bool TB>
-__device__ inline void gemm(int M, int N, int K, double alpha, const double* A, long lda, const double* B, long ldb,
-                     double beta, double* C, long ldc, LaSmem& sm) {
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+// Warp tile: 32 rows x 16 columns of the 64 x 64 CTA tile.
+template <typename T>
+struct Acc;
+template <>
+struct Acc<double> {
+    double v[4][2][2];  // 4 (m8) x 2 (n8) fragments of m8n8
+};
+template <>
+struct Acc<float> {
+    float v[2][2][4];  // 2 (m16) x 2 (n8) fragments of m16n8
+};
+
+__device__ __forceinline__ void acc_zero(Acc<double>& a) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) a.v[i][j][0] = a.v[i][j][1] = 0.0;
+}
+__device__ __forceinline__ void acc_zero(Acc<float>& a) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a.v[i][j][q] = 0.f;
+}
+
+// one TK-deep step of the warp tile from the staged tiles
+__device__ __forceinline__ void warp_step(Acc<double>& acc, const LaSmem<double>& sm, int wm, int wn, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int k4 = 0; k4 < TK; k4 += 4) {
+        double a[4], b[2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = sm.A[k4 + t][wm + 8 * i + g];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) b[j] = sm.B[k4 + t][wn + 8 * j + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) mma_f64(acc.v[i][j], a[i], b[j]);
+    }
+}
+
+__device__ __forceinline__ void warp_step(Acc<float>& acc, const LaSmem<float>& sm, int wm, int wn, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int k8 = 0; k8 < TK; k8 += 8) {
+        uint32_t ah[2][4], al[2][4], bh[2][2], bl[2][2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r0 = wm + 16 * i + g;
+            float x[4] = {sm.A[k8 + t][r0], sm.A[k8 + t][r0 + 8], sm.A[k8 + t + 4][r0], sm.A[k8 + t + 4][r0 + 8]};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ah[i][q] = to_tf32(x[q]);
+                al[i][q] = to_tf32(x[q] - __uint_as_float(ah[i][q]));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int c0 = wn + 8 * j + g;
+            float y[2] = {sm.B[k8 + t][c0], sm.B[k8 + t + 4][c0]};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                bh[j][q] = to_tf32(y[q]);
+                bl[j][q] = to_tf32(y[q] - __uint_as_float(bh[j][q]));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                mma_tf32(acc.v[i][j], al[i], bh[j]);
+                mma_tf32(acc.v[i][j], ah[i], bl[j]);
+                mma_tf32(acc.v[i][j], ah[i], bh[j]);
+            }
+    }
+}
+
+// write back: C = alpha*acc + beta*C for the warp tile
+template <typename T>
+__device__ __forceinline__ void put(T* C, long ldc, int M, int N, int r, int c, T alpha, T beta, T v) {
+    if (r < M && c < N) {
+        T* p = C + r + (long)c * ldc;
+        *p = beta == (T)0 ? alpha * v : alpha * v + beta * *p;
+    }
+}
+__device__ __forceinline__ void acc_store(const Acc<double>& acc, double* C, long ldc, int M, int N, int m0, int n0,
+                                          int wm, int wn, int lane, double alpha, double beta) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int r = m0 + wm + 8 * i + g, c = n0 + wn + 8 * j + 2 * t;
+            put(C, ldc, M, N, r, c, alpha, beta, acc.v[i][j][0]);
+            put(C, ldc, M, N, r, c + 1, alpha, beta, acc.v[i][j][1]);
+        }
+}
+__device__ __forceinline__ void acc_store(const Acc<float>& acc, float* C, long ldc, int M, int N, int m0, int n0,
+                                          int wm, int wn, int lane, float alpha, float beta) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * t;
+            put(C, ldc, M, N, r, c, alpha, beta, acc.v[i][j][0]);
+            put(C, ldc, M, N, r, c + 1, alpha, beta, acc.v[i][j][1]);
+            put(C, ldc, M, N, r + 8, c, alpha, beta, acc.v[i][j][2]);
+            put(C, ldc, M, N, r + 8, c + 1, alpha, beta, acc.v[i][j][3]);
+        }
+}
+
+// C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N, column-major,
+// any leading dimensions, global or shared memory.  beta == 0 never reads C.
+// The next TK-deep slab is fetched into registers while the tensor pipe works
+// on the current one.  Ends with a barrier.
+template <typename T, bool TA, bool TB>
+__device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta, T* C,
+                            long ldc, LaSmem<T>& sm) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
+    constexpr int PER = TK * TM / kThreads;  // elements of each operand per thread per slab (4)
     for (int m0 = 0; m0 < M; m0 += TM) {
         for (int n0 = 0; n0 < N; n0 += TN) {
-            double acc[4][4];
+            Acc<T> acc;
+            acc_zero(acc);
+            T ra[PER], rb[PER];
+            auto fetch = [&](int k0) {
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-            for (int k0 = 0; k0 < K; k0 += TK) {
-#pragma unroll
-                for (int e = tid; e < TK * TM; e += kThreads) {
+                for (int q = 0; q < PER; ++q) {
+                    const int e = tid + q * kThreads;
                     int i, k;
                     if (!TA) { i = e % TM; k = e / TM; } else { k = e % TK; i = e / TK; }
-                    int gi = m0 + i, gk = k0 + k;
-                    double v = 0.0;
-                    if (gi < M && gk < K) v = TA ? A[gk + (long)gi * lda] : A[gi + (long)gk * lda];
-                    sm.A[k][i] = v;
+                    const int gi = m0 + i, gk = k0 + k;
+                    ra[q] = (gi < M && gk < K) ? (TA ? A[gk + (long)gi * lda] : A[gi + (long)gk * lda]) : (T)0;
+                    int j, kb;
+                    if (!TB) { kb = e % TK; j = e / TK; } else { j = e % TN; kb = e / TN; }
+                    const int gj = n0 + j, gkb = k0 + kb;
+                    rb[q] = (gj < N && gkb < K) ? (TB ? B[gj + (long)gkb * ldb] : B[gkb + (long)gj * ldb]) : (T)0;
                 }
+            };
+            auto stash = [&]() {
 #pragma unroll
-                for (int e = tid; e < TK * TN; e += kThreads) {
-                    int j, k;
-                    if (!TB) { k = e % TK; j = e / TK; } else { j = e % TN; k = e / TN; }
-                    int gj = n0 + j, gk = k0 + k;
-                    double v = 0.0;
-                    if (gj < N && gk < K) v = TB ? B[gj + (long)gk * ldb] : B[gk + (long)gj * ldb];
-                    sm.B[k][j] = v;
+                for (int q = 0; q < PER; ++q) {
+                    const int e = tid + q * kThreads;
+                    int i, k;
+                    if (!TA) { i = e % TM; k = e / TM; } else { k = e % TK; i = e / TK; }
+                    sm.A[k][i] = ra[q];
+                    int j, kb;
+                    if (!TB) { kb = e % TK; j = e / TK; } else { j = e % TN; kb = e / TN; }
+                    sm.B[kb][j] = rb[q];
                 }
-                __syncthreads();
-#pragma unroll
-                for (int kk = 0; kk < TK; ++kk) {
-                    double a[4], b[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) a[q] = sm.A[kk][tx + 16 * q];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) b[q] = sm.B[kk][ty + 16 * q];
-#pragma unroll
-                    for (int x = 0; x < 4; ++x)
-#pragma unroll
-                        for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
-                }
-                __syncthreads();
+            };
+            if (K > 0) {
+                fetch(0);
+                stash();
             }
-#pragma unroll
-            for (int x = 0; x < 4; ++x) {
-                int gi = m0 + tx + 16 * x;
-                if (gi >= M) continue;
-#pragma unroll
-                for (int y = 0; y < 4; ++y) {
-                    int gj = n0 + ty + 16 * y;
-                    if (gj >= N) continue;
-                    double* c = C + gi + (long)gj * ldc;
-                    *c = beta == 0.0 ? alpha * acc[x][y] : fma(alpha, acc[x][y], beta * *c);
+            __syncthreads();
+            for (int k0 = 0; k0 < K; k0 += TK) {
+                const bool more = k0 + TK < K;
+                if (more) fetch(k0 + TK);
+                warp_step(acc, sm, wm, wn, lane);
+                __syncthreads();
+                if (more) {
+                    stash();
+                    __syncthreads();
                 }
             }
+            acc_store(acc, C, ldc, M, N, m0, n0, wm, wn, lane, alpha, beta);
         }
     }
     __syncthreads();
 }
 
 // B <- L^{-1} B  (L: n x n lower, non-unit; B: n x nrhs).  dtrtrs('L','N','N').
-__device__ inline void trsm_left_lower(int n, int nrhs, const double* L, long ldl, double* B, long ldb, LaSmem& sm) {
+// Diagonal blocks are solved in FP64; trailing updates go through gemm<T>.
+template <typename T>
+__device__ inline void trsm_left_lower(int n, int nrhs, const T* L, long ldl, T* B, long ldb, LaSmem<T>& sm) {
     const int tid = threadIdx.x;
     for (int b0 = 0; b0 < n; b0 += NB) {
         int nb = min(NB, n - b0);
         for (int e = tid; e < nb * nb; e += kThreads) {
             int i = e % nb, j = e / nb;
-            sm.D[i][j] = L[(b0 + i) + (long)(b0 + j) * ldl];
+            sm.D[i][j] = (double)L[(b0 + i) + (long)(b0 + j) * ldl];
         }
         __syncthreads();
         for (int c = tid; c < nrhs; c += kThreads) {
             double x[NB];
-            double* col = B + b0 + (long)c * ldb;
+            T* col = B + b0 + (long)c * ldb;
 #pragma unroll
-            for (int i = 0; i < NB; ++i) x[i] = i < nb ? col[i] : 0.0;
+            for (int i = 0; i < NB; ++i) x[i] = i < nb ? (double)col[i] : 0.0;
 #pragma unroll
             for (int i = 0; i < NB; ++i) {
                 if (i < nb) {
@@ -200,31 +385,31 @@ __device__ inline void trsm_left_lower(int n, int nrhs, const double* L, long ld
             }
 #pragma unroll
             for (int i = 0; i < NB; ++i)
-                if (i < nb) col[i] = x[i];
+                if (i < nb) col[i] = (T)x[i];
         }
         __syncthreads();
         if (b0 + nb < n)
-            gemm<false, false>(n - b0 - nb, nrhs, nb, -1.0, L + (b0 + nb) + (long)b0 * ldl, ldl, B + b0, ldb, 1.0,
-                               B + b0 + nb, ldb, sm);
+            gemm<T, false, false>(n - b0 - nb, nrhs, nb, (T)-1, L + (b0 + nb) + (long)b0 * ldl, ldl, B + b0, ldb,
+                                  (T)1, B + b0 + nb, ldb, sm);
     }
 }
 
 // B <- B L^{-T}  (L: n x n lower; B: rows x n).  Row-wise forward substitution.
-__device__ inline void trsm_right_lower_trans(int rows, int n, const double* L, long ldl, double* B, long ldb,
-                                       LaSmem& sm) {
+template <typename T>
+__device__ inline void trsm_right_lower_trans(int rows, int n, const T* L, long ldl, T* B, long ldb, LaSmem<T>& sm) {
     const int tid = threadIdx.x;
     for (int b0 = 0; b0 < n; b0 += NB) {
         int nb = min(NB, n - b0);
         for (int e = tid; e < nb * nb; e += kThreads) {
             int i = e % nb, j = e / nb;
-            sm.D[i][j] = L[(b0 + i) + (long)(b0 + j) * ldl];
+            sm.D[i][j] = (double)L[(b0 + i) + (long)(b0 + j) * ldl];
         }
         __syncthreads();
         for (int row = tid; row < rows; row += kThreads) {
             double x[NB];
-            double* p = B + row + (long)b0 * ldb;
+            T* p = B + row + (long)b0 * ldb;
 #pragma unroll
-            for (int i = 0; i < NB; ++i) x[i] = i < nb ? p[(long)i * ldb] : 0.0;
+            for (int i = 0; i < NB; ++i) x[i] = i < nb ? (double)p[(long)i * ldb] : 0.0;
 #pragma unroll
             for (int i = 0; i < NB; ++i) {
                 if (i < nb) {
@@ -236,27 +421,48 @@ __device__ inline void trsm_right_lower_trans(int rows, int n, const double* L, 
             }
 #pragma unroll
             for (int i = 0; i < NB; ++i)
-                if (i < nb) p[(long)i * ldb] = x[i];
+                if (i < nb) p[(long)i * ldb] = (T)x[i];
         }
         __syncthreads();
         if (b0 + nb < n)
-            gemm<false, true>(rows, n - b0 - nb, nb, -1.0, B + (long)b0 * ldb, ldb, L + (b0 + nb) + (long)b0 * ldl,
-                              ldl, 1.0, B + (long)(b0 + nb) * ldb, ldb, sm);
+            gemm<T, false, true>(rows, n - b0 - nb, nb, (T)-1, B + (long)b0 * ldb, ldb, L + (b0 + nb) + (long)b0 * ldl,
+                                 ldl, (T)1, B + (long)(b0 + nb) * ldb, ldb, sm);
     }
 }
 
+// Solves L x = b for one right-hand side entirely in FP64 (the vectors that feed
+// quadratic forms), x overwrites b.  Single warp does the work; ends with a barrier.
+template <typename T>
+__device__ inline void trsv_lower_f64(int n, const T* L, long ldl, double* b) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int k = lane; k < i; k += 32) s += (double)L[i + (long)k * ldl] * b[k];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) b[i] = (b[i] - s) / (double)L[i + (long)i * ldl];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+}
+
 // In-place lower Cholesky A = L L^T (strict upper part zeroed, like
-// Armadillo's chol(X, "lower")).  Returns 0, or the 1-based index of the
-// first non-positive pivot (LAPACK dpotrf's info); the factorization then
-// continues on NaNs and the caller reports the region.
-__device__ inline int potrf_lower(int n, double* A, long lda, LaSmem& sm) {
+// Armadillo's chol(X, "lower")).  Diagonal blocks and panels in FP64, trailing
+// updates through gemm<T>.  Returns 0, or the 1-based index of the first
+// non-positive (or NaN) pivot (LAPACK's info); the factorization then goes on
+// with NaNs and the caller reports the region.  *logdet (thread 0) receives
+// 2 * sum(log(diag L)) accumulated in FP64.
+template <typename T>
+__device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* logdet) {
     const int tid = threadIdx.x;
+    double ld = 0.0;
     if (tid == 0) sm.flag = 0;
     for (int b0 = 0; b0 < n; b0 += NB) {
         int nb = min(NB, n - b0);
         for (int e = tid; e < nb * nb; e += kThreads) {
             int i = e % nb, j = e / nb;
-            sm.D[i][j] = A[(b0 + i) + (long)(b0 + j) * lda];
+            sm.D[i][j] = (double)A[(b0 + i) + (long)(b0 + j) * lda];
         }
         __syncthreads();
         for (int k = 0; k < nb; ++k) {
@@ -264,6 +470,7 @@ __device__ inline int potrf_lower(int n, double* A, long lda, LaSmem& sm) {
                 double d = sm.D[k][k];
                 if (!(d > 0.0) && sm.flag == 0) sm.flag = b0 + k + 1;
                 sm.D[k][k] = sqrt(d);
+                ld += 2.0 * log(sm.D[k][k]);
             }
             __syncthreads();
             double dk = sm.D[k][k];
@@ -278,17 +485,17 @@ __device__ inline int potrf_lower(int n, double* A, long lda, LaSmem& sm) {
         }
         for (int e = tid; e < nb * nb; e += kThreads) {
             int i = e % nb, j = e / nb;
-            A[(b0 + i) + (long)(b0 + j) * lda] = j <= i ? sm.D[i][j] : 0.0;
+            A[(b0 + i) + (long)(b0 + j) * lda] = j <= i ? (T)sm.D[i][j] : (T)0;
         }
         __syncthreads();
         int rest = n - b0 - nb;
         if (rest > 0) {
-            // panel: A[b0+nb:, b0:b0+nb] <- A[...] * D^{-T}
+            // panel: A[b0+nb:, b0:b0+nb] <- A[...] * D^{-T}, in FP64
             for (int row = tid; row < rest; row += kThreads) {
                 double x[NB];
-                double* p = A + (b0 + nb + row) + (long)b0 * lda;
+                T* p = A + (b0 + nb + row) + (long)b0 * lda;
 #pragma unroll
-                for (int i = 0; i < NB; ++i) x[i] = i < nb ? p[(long)i * lda] : 0.0;
+                for (int i = 0; i < NB; ++i) x[i] = i < nb ? (double)p[(long)i * lda] : 0.0;
 #pragma unroll
                 for (int i = 0; i < NB; ++i) {
                     if (i < nb) {
@@ -300,26 +507,27 @@ __device__ inline int potrf_lower(int n, double* A, long lda, LaSmem& sm) {
                 }
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
-                    if (i < nb) p[(long)i * lda] = x[i];
+                    if (i < nb) p[(long)i * lda] = (T)x[i];
             }
             __syncthreads();
-            const double* P = A + (b0 + nb) + (long)b0 * lda;
-            gemm<false, true>(rest, rest, nb, -1.0, P, lda, P, lda, 1.0, A + (b0 + nb) + (long)(b0 + nb) * lda, lda,
-                              sm);
-            // the strict upper part of the trailing block is scratch; zero it
+            const T* P = A + (b0 + nb) + (long)b0 * lda;
+            gemm<T, false, true>(rest, rest, nb, (T)-1, P, lda, P, lda, (T)1, A + (b0 + nb) + (long)(b0 + nb) * lda,
+                                 lda, sm);
             for (int e = tid; e < nb * rest; e += kThreads) {
                 int i = e % nb, j = e / nb;
-                A[(b0 + i) + (long)(b0 + nb + j) * lda] = 0.0;
+                A[(b0 + i) + (long)(b0 + nb + j) * lda] = (T)0;
             }
             __syncthreads();
         }
     }
     __syncthreads();
+    if (tid == 0 && logdet) *logdet = ld;
     return sm.flag;
 }
 
 // Deterministic CTA sum (fixed thread -> element mapping and tree order).
-__device__ inline double cta_sum(double v, LaSmem& sm) {
+template <typename T>
+__device__ inline double cta_sum(double v, LaSmem<T>& sm) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
     __syncthreads();

@@ -1,24 +1,38 @@
-// FP64 region kernels of the MRA hot path.
+// Region kernels of the MRA hot path, templated on the storage type T
+// (double: plain FP64 path; float: mixed path, FP32 storage and 3xTF32 tensor
+// products, FP64 diagonal blocks and log-likelihood accumulation).
 //
-// Level-synchronous schedule (one launch per tree level and stage):
-//   k_fields          sigma^2/beta/tau^2 at every knot, observation and
-//                     prediction point (class_nonstationary_covariance.cpp:479-573)
-//   k_prior_level(m)  one CTA per level-m region: U_{i,j} = L_{a_j}^{-1} V_j and
-//                     L_i = chol(K_i)   (class_approximation.cpp:84-169)
-//   k_finest          one CTA per finest region, largest first from a work
-//                     queue: U, Sigma_i, L_Sigma, y~, B^, log-lik terms
-//                     (...-loop-regions-at-finest-level-in-prior.cpp:90-269)
-//   k_posterior(m)    levels M-2..0: child sums, L~ = chol(L L^T + A), v, G,
-//                     w~, A~   (...-posterior-inference.cpp:14-265,
-//                     class_approximation.cpp:186-306)
-//   k_predict         one CTA per finest region with predictions: prior half
-//                     (...-prior.cpp:271-392) then the top-down pass
-//                     (class_approximation-predict.cpp:105-189)
-//   k_reduce          deterministic sum of the per-region log-lik terms
+// Schedule of one log-likelihood (one launch per stage and tree level):
+//   k_fields            sigma^2/beta/tau^2 at every knot, observation and
+//                       prediction point (class_nonstationary_covariance.cpp:479-573)
+//   k_prior_level(m)    levels 0..M-2, one CTA per region: U_{i,j} = L_{a_j}^{-1} V_j,
+//                       L_i = chol(K_i)   (class_approximation.cpp:46-50,84-169)
+//   k_finest_group      one CTA per level M-2 region, its finest children as one
+//                       sibling group: conditioning of all their observations on
+//                       the shared ancestors, then per child Sigma, L_Sigma, y~,
+//                       B^ and the log-lik terms
+//                       (...-loop-regions-at-finest-level-in-prior.cpp:90-269),
+//                       then the level M-2 posterior of the parent
+//   k_posterior_level(m) levels M-3..0 (...-posterior-inference.cpp:14-265,
+//                       class_approximation.cpp:186-306)
+//   k_reduce            deterministic sum of the per-region terms
+//   k_predict           prediction, one CTA per finest region with predictions
+//                       (...-prior.cpp:271-392, class_approximation-predict.cpp:105-189)
 //
-// Finest-level A~ slices are never materialised: the level M-2 posterior forms
-// the children's sum sum_c B^_{c,j}^T B^_{c,k} directly as one product over the
-// stacked observation rows of its children.
+// Posterior representation.  A region's contribution to its parent is the pair
+// (A~, w~) of the reference (class_approximation.cpp:266-306).  Below a size
+// threshold it is carried in factored observation-space form instead: a matrix
+// F (n x m r, one row per observation of the subtree) and a vector f with
+// A~_(j,k) = F_j^T F_k and w~_j = F_j^T f.  The finest level starts in this
+// form (F = B^, f = y~).  For a region i at level m with factored input (F, f):
+//   Y = L_i^{-1} F_m^T,  R R^T = I + Y^T Y,
+//   output F' = R^{-1} F_{0..m-1},  f' = R^{-1} f,
+//   log-lik term 2 log|R| - (f^T f - f'^T f'),
+// which equals the reference's -2 log|L_i| + 2 log|L~_i| - v^T v with
+// L~ L~^T = L L^T + F_m^T F_m (Sylvester's determinant identity and Woodbury),
+// and F'^T F' / F'^T f' equal the reference's A~ / w~ of the region.  Larger
+// regions use the reference's dense r x r slices.  Prediction mode also forms
+// L~, v and G of factored regions from (F, f).
 #include "mra_kernels.cuh"
 
 namespace mra {
@@ -74,8 +88,9 @@ __global__ void k_fields(Geom g, FieldParams fp, const double* __restrict__ c0, 
 // ---------------------------------------------------------------------------
 // a5/a6: prior, one level of interior regions
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree t, int m) {
-    __shared__ LaSmem sm;
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> t, int m) {
+    __shared__ LaSmem<T> sm;
     const int r = t.r;
     const long rr = (long)r * r;
     const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
@@ -90,186 +105,357 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree t, 
                 anc[a] = c;
             }
         }
-        double* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
+        T* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            double* V = Ui + (long)j * r;
-            fill_cov(g, t.pts, a * r, r, i * r, r, false, V, mr);
+            T* V = Ui + (long)j * r;
+            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, mr);
             __syncthreads();
             if (j > 0) {
-                const double* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<true, false>(r, r, j * r, -1.0, Ua, (long)j * r, Ui, mr, 1.0, V, mr, sm);
+                const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
+                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, mr, sm);
             }
-            trsm_left_lower(r, r, t.Lprior + a * rr, r, V, mr, sm);
+            trsm_left_lower<T>(r, r, t.Lprior + a * rr, r, V, mr, sm);
         }
-        double* Li = t.Lprior + i * rr;
-        fill_cov(g, t.pts, i * r, r, i * r, r, true, Li, r);
+        T* Li = t.Lprior + i * rr;
+        fill_cov<T>(g, t.pts, i * r, r, i * r, r, true, Li, r);
         __syncthreads();
-        if (m > 0) gemm<true, false>(r, r, (int)mr, -1.0, Ui, mr, Ui, mr, 1.0, Li, r, sm);
-        int info = potrf_lower(r, Li, r, sm);
-        if (info && threadIdx.x == 0) report_error(t.err, i);
+        if (m > 0) gemm<T, true, false>(r, r, (int)mr, (T)-1, Ui, mr, Ui, mr, (T)1, Li, r, sm);
+        double ld = 0.0;
+        int info = potrf_lower<T>(r, Li, r, sm, &ld);
+        if (threadIdx.x == 0) {
+            t.ldprior[i] = ld;
+            if (info) report_error(t.err, i);
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// a7/a8: prior at the finest level
+// posterior steps of one region (level m): factored and dense forms
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2) k_finest(Geom g, DevTree t) {
-    __shared__ LaSmem sm;
-    __shared__ long s_k;
-    const int r = t.r, L = t.L;
+// Factored input (F: n rows of width (m+1) r, row stride ldF; f: n doubles).
+// Writes F' (n rows of width m r) to Fo and f' to fo when m > 0.
+template <typename T>
+__device__ void factored_step(const DevTree<T>& t, int m, long i, int n, const T* F, long ldF, const double* f, T* Fo,
+                              double* fo, bool keep, T* ws, double* wsd, LaSmem<T>& sm, double& dterm) {
+    const int r = t.r;
+    const long rr = (long)r * r, mr = (long)m * r;
+    const T* Li = t.Lprior + i * rr;
+    T* Y = ws;                  // r x n
+    T* S = ws + (long)r * n;    // n x n
+    for (long e = threadIdx.x; e < (long)r * n; e += kThreads) {
+        int tt = (int)(e % r), q = (int)(e / r);
+        Y[e] = F[(long)q * ldF + mr + tt];
+    }
+    __syncthreads();
+    trsm_left_lower<T>(r, n, Li, r, Y, r, sm);
+    gemm<T, true, false>(n, n, r, (T)1, Y, r, Y, r, (T)0, S, n, sm);
+    for (int q = threadIdx.x; q < n; q += kThreads) S[q + (long)q * n] += (T)1;
+    __syncthreads();
+    double ld = 0.0;
+    int info = potrf_lower<T>(n, S, n, sm, &ld);
+    double* fp = m > 0 ? fo : wsd;
+    double part = 0.0;
+    for (int q = threadIdx.x; q < n; q += kThreads) {
+        fp[q] = f[q];
+        part += f[q] * f[q];
+    }
+    double ff = cta_sum(part, sm);
+    trsv_lower_f64<T>(n, S, n, fp);
+    part = 0.0;
+    for (int q = threadIdx.x; q < n; q += kThreads) part += fp[q] * fp[q];
+    double pp = cta_sum(part, sm);
+    if (threadIdx.x == 0) {
+        dterm += ld - (ff - pp);
+        if (info) report_error(t.err, i);
+    }
+    if (m > 0) {
+        for (long e = threadIdx.x; e < mr * n; e += kThreads) {
+            long x = e % mr, q = e / mr;
+            Fo[q * mr + x] = F[q * ldF + x];
+        }
+        __syncthreads();
+        trsm_right_lower_trans<T>((int)mr, n, S, n, Fo, mr, sm);
+    }
+    if (keep) {
+        // predictive factors of the region: L~ L~^T = L L^T + F_m^T F_m, v = L~^{-1} F_m^T f,
+        // G = L~^{-1} F_m^T F_{0..m-1}
+        T* Lt = t.Lpost + i * rr;
+        gemm<T, false, true>(r, r, r, (T)1, Li, r, Li, r, (T)0, Lt, r, sm);
+        gemm<T, false, true>(r, r, n, (T)1, F + mr, ldF, F + mr, ldF, (T)1, Lt, r, sm);
+        int info2 = potrf_lower<T>(r, Lt, r, sm, nullptr);
+        double* v = t.vpost + i * r;
+        for (int tt = threadIdx.x; tt < r; tt += kThreads) {
+            double s = 0.0;
+            for (int q = 0; q < n; ++q) s += (double)F[(long)q * ldF + mr + tt] * f[q];
+            v[tt] = s;
+        }
+        __syncthreads();
+        trsv_lower_f64<T>(r, Lt, r, v);
+        if (m > 0) {
+            T* Gi = t.G + t.u_off[m] + (i - level_start(t.J, m)) * mr * r;
+            gemm<T, false, true>(r, (int)mr, n, (T)1, F + mr, ldF, F, ldF, (T)0, Gi, r, sm);
+            trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
+        }
+        if (info2 && threadIdx.x == 0) report_error(t.err, i);
+    }
+}
+
+// Dense input: Aagg holds the slices (j,k), j <= k <= m, of the summed children
+// contributions, wagg the (m+1) x r summed w.
+template <typename T>
+__device__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, const double* wagg, bool keep, T* Gw,
+                           LaSmem<T>& sm, double& dterm) {
+    const int r = t.r;
+    const long rr = (long)r * r, mr = (long)m * r;
+    const long loc = i - level_start(t.J, m);
+    const T* Lp = t.Lprior + i * rr;
+    T* Lt = t.Lpost + i * rr;
+    gemm<T, false, true>(r, r, r, (T)1, Lp, r, Lp, r, (T)0, Lt, r, sm);
+    const T* Amm = Aagg + slice_index(m + 1, m, m) * rr;
+    for (long e = threadIdx.x; e < rr; e += kThreads) Lt[e] += Amm[e];
+    __syncthreads();
+    double ld = 0.0;
+    int info = potrf_lower<T>(r, Lt, r, sm, &ld);
+    double* v = t.vpost + i * r;
+    for (int e = threadIdx.x; e < r; e += kThreads) v[e] = wagg[mr + e];
+    __syncthreads();
+    trsv_lower_f64<T>(r, Lt, r, v);
+    double part = 0.0;
+    for (int e = threadIdx.x; e < r; e += kThreads) part += v[e] * v[e];
+    double vv = cta_sum(part, sm);
+    if (threadIdx.x == 0) {
+        dterm += ld - t.ldprior[i] - vv;
+        if (info) report_error(t.err, i);
+    }
+    if (m == 0) return;
+    T* Gi = keep ? t.G + t.u_off[m] + loc * mr * r : Gw;  // r x (m r), ld = r
+    for (long e = threadIdx.x; e < mr * r; e += kThreads) {
+        int j = (int)(e / rr);
+        long w = e % rr;
+        int p = (int)(w % r), q = (int)(w / r);
+        Gi[e] = Aagg[slice_index(m + 1, j, m) * rr + q + (long)p * r];  // G_j = A_(j,m)^T
+    }
+    __syncthreads();
+    trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
+    double* wo = t.wout[m & 1] + loc * mr;
+    for (long x = threadIdx.x; x < mr; x += kThreads) {
+        double s = 0.0;
+        for (int tt = 0; tt < r; ++tt) s += (double)Gi[tt + x * r] * v[tt];
+        wo[x] = wagg[x] - s;
+    }
+    T* ao = t.aout[m & 1] + loc * n_slices(m) * rr;
+    for (int j = 0; j < m; ++j) {
+        for (int k = j; k < m; ++k) {
+            T* dst = ao + slice_index(m, j, k) * rr;
+            const T* src = Aagg + slice_index(m + 1, j, k) * rr;
+            for (long e = threadIdx.x; e < rr; e += kThreads) dst[e] = src[e];
+            __syncthreads();
+            gemm<T, true, false>(r, r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)k * rr, r, (T)1, dst, r, sm);
+        }
+    }
+}
+
+// Aagg/wagg += the (A~, w~) of factored rows F (n x (m+1) r, row stride ldF), f.
+template <typename T>
+__device__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* F, long ldF, const double* f, T* Aagg,
+                                    double* wagg, LaSmem<T>& sm) {
+    const int r = t.r;
+    const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
+    if (n == 0) return;
+    for (int j = 0; j <= m; ++j)
+        for (int k = j; k <= m; ++k)
+            gemm<T, false, true>(r, r, n, (T)1, F + (long)j * r, ldF, F + (long)k * r, ldF, (T)1,
+                                 Aagg + slice_index(m + 1, j, k) * rr, r, sm);
+    for (long x = threadIdx.x; x < mr1; x += kThreads) {
+        double s = 0.0;
+        for (int q = 0; q < n; ++q) s += (double)F[(long)q * ldF + x] * f[q];
+        wagg[x] += s;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// a7/a8 (+ a9 at level M-2): finest level, one CTA per sibling group
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T> t, int keep) {
+    __shared__ LaSmem<T> sm;
+    __shared__ long s_p;
+    const int r = t.r, L = t.L, m = t.M - 2;
     const long rr = (long)r * r, Lr = (long)L * r;
+    const long s2 = level_start(t.J, m), cnt2 = level_count(t.J, m);
+    T* ws = t.ws + blockIdx.x * t.ws_stride;
+    double* wsd = t.wsd + blockIdx.x * t.wsd_stride;
     for (;;) {
         if (threadIdx.x == 0) {
             int q = atomicAdd(&t.queue[0], 1);
-            s_k = q < t.n_fin ? t.fin_order[q] : -1;
+            s_p = q < cnt2 ? t.par_order[q] : -1;
         }
         __syncthreads();
-        const long k = s_k;
+        const long ploc = s_p;
         __syncthreads();
-        if (k < 0) break;
-        const long o0 = t.obs_off[k];
-        const int n = (int)(t.obs_off[k + 1] - o0);
-        if (n == 0) {
-            if (threadIdx.x == 0) t.dfin[k] = 0.0;
-            continue;
-        }
-        const int64_t* anc = t.fin_anc + k * L;
-        double* Uf = t.Ufin + o0 * Lr;  // (L r) x n, ld = L r
-        double* Bh = t.Bhat + o0 * Lr;  // (L r) x n, ld = L r  (= B^ transposed)
-        for (int j = 0; j < L; ++j) {
-            const long a = anc[j];
-            double* V = Uf + (long)j * r;
-            fill_cov(g, t.pts, a * r, r, t.obs0 + o0, n, false, V, Lr);
-            __syncthreads();
-            if (j > 0) {
-                const double* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<true, false>(r, n, j * r, -1.0, Ua, (long)j * r, Uf, Lr, 1.0, V, Lr, sm);
+        if (ploc < 0) break;
+        const long p = s2 + ploc;
+        const long clo = t.child_lo[ploc], chi = t.child_hi[ploc];
+        const long lo = t.obs_off[clo];
+        const int np = (int)(t.obs_off[chi] - lo);
+        long anc[kMaxLevels];
+        anc[m] = p;
+        {
+            long c = p;
+            for (int a = m - 1; a >= 0; --a) {
+                c = (c - 1) / t.J;
+                anc[a] = c;
             }
-            for (int e = threadIdx.x; e < r * n; e += kThreads) {
-                int tt = e % r, q = e / r;
-                Bh[(long)j * r + tt + (long)q * Lr] = V[tt + (long)q * Lr];
+        }
+        double dterm = 0.0;
+        if (np > 0) {
+            T* Uf = t.Ufin + lo * Lr;  // (L r) x np, ld = L r
+            T* Bh = t.Bhat + lo * Lr;
+            for (int j = 0; j < L; ++j) {
+                const long a = anc[j];
+                T* V = Uf + (long)j * r;
+                fill_cov<T>(g, t.pts, a * r, r, t.obs0 + lo, np, false, V, Lr);
+                __syncthreads();
+                if (j > 0) {
+                    const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
+                    gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, Uf, Lr, (T)1, V, Lr, sm);
+                }
+                for (long e = threadIdx.x; e < (long)r * np; e += kThreads) {
+                    int tt = (int)(e % r);
+                    long q = e / r;
+                    Bh[(long)j * r + tt + q * Lr] = V[tt + q * Lr];
+                }
+                __syncthreads();
+                trsm_left_lower<T>(r, np, t.Lprior + a * rr, r, V, Lr, sm);
             }
+            for (long c = clo; c < chi; ++c) {
+                const long o0 = t.obs_off[c];
+                const int n = (int)(t.obs_off[c + 1] - o0);
+                if (n == 0) continue;
+                T* S = t.Lsig + t.lsig_off[c];
+                fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n);
+                __syncthreads();
+                gemm<T, true, false>(n, n, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, t.Ufin + o0 * Lr, Lr, (T)1, S, n,
+                                     sm);
+                double ld = 0.0;
+                int info = potrf_lower<T>(n, S, n, sm, &ld);
+                double* ytc = t.yt + o0;
+                for (int e = threadIdx.x; e < n; e += kThreads) ytc[e] = t.y[o0 + e];
+                __syncthreads();
+                trsv_lower_f64<T>(n, S, n, ytc);
+                trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
+                double part = 0.0;
+                for (int e = threadIdx.x; e < n; e += kThreads) part += ytc[e] * ytc[e];
+                double yy = cta_sum(part, sm);
+                if (threadIdx.x == 0) {
+                    dterm += yy + ld;
+                    if (info) report_error(t.err, t.n_int + c);
+                }
+            }
+        }
+        if (threadIdx.x == 0) t.dfin[ploc] = dterm;
+        if (!t.fuse_post) continue;
+        dterm = 0.0;
+        // posterior of the parent at level m = M-2 from F = B^ rows, f = y~
+        const T* F = t.Bhat + lo * Lr;
+        const double* f = t.yt + lo;
+        if (t.factored[p]) {
+            T* Fo = m > 0 ? t.Fbuf[m & 1] + lo * (long)m * r : nullptr;
+            double* fo = m > 0 ? t.fbuf[m & 1] + lo : nullptr;
+            factored_step<T>(t, m, p, np, F, Lr, f, Fo, fo, keep != 0, ws, wsd, sm, dterm);
+        } else {
+            T* Aagg = ws;
+            double* wagg = wsd;
+            for (long e = threadIdx.x; e < n_slices(m + 1) * rr; e += kThreads) Aagg[e] = (T)0;
+            for (long e = threadIdx.x; e < Lr; e += kThreads) wagg[e] = 0.0;
             __syncthreads();
-            trsm_left_lower(r, n, t.Lprior + a * rr, r, V, Lr, sm);
+            accumulate_factored<T>(t, m, np, F, Lr, f, Aagg, wagg, sm);
+            dense_step<T>(t, m, p, Aagg, wagg, keep != 0, Aagg + n_slices(m + 1) * rr, sm, dterm);
         }
-        double* S = t.Lsig + t.lsig_off[k];
-        fill_cov(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n);
+        if (threadIdx.x == 0) t.dpost[p] = dterm;
         __syncthreads();
-        gemm<true, false>(n, n, (int)Lr, -1.0, Uf, Lr, Uf, Lr, 1.0, S, n, sm);
-        int info = potrf_lower(n, S, n, sm);
-        double* yt = t.yt + o0;
-        for (int e = threadIdx.x; e < n; e += kThreads) yt[e] = t.y[o0 + e];
-        __syncthreads();
-        trsm_left_lower(n, 1, S, n, yt, n, sm);
-        trsm_right_lower_trans((int)Lr, n, S, n, Bh, Lr, sm);
-        double part = 0.0;
-        for (int e = threadIdx.x; e < n; e += kThreads) part += yt[e] * yt[e] + 2 * log(S[e + (long)e * n]);
-        double tot = cta_sum(part, sm);
-        if (threadIdx.x == 0) {
-            t.dfin[k] = tot;
-            if (info) report_error(t.err, t.n_int + k);
-        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// a9/a10/a11/a14: posterior, one level (m = M-2 .. 0)
+// a9/a10/a11: posterior, one level (m = M-3 .. 0)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree t, int m, int keep_g) {
-    __shared__ LaSmem sm;
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree<T> t, int m, int keep) {
+    __shared__ LaSmem<T> sm;
     const int r = t.r;
-    const long rr = (long)r * r;
+    const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
     const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
-    const long ns_in = n_slices(m + 1), ns_out = n_slices(m);
-    const long mr1 = (long)(m + 1) * r;
-    double* ws = t.ws + blockIdx.x * t.ws_stride;
-    double* Aagg = ws;               // ns_in slices of r x r
-    double* wagg = Aagg + ns_in * rr;  // (m+1) x r
-    double* Gw = wagg + mr1;         // m slices, when G is not kept
-    const double* ain = t.aout[(m + 1) & 1];
+    const long s1 = level_start(t.J, m + 1);
+    const long ns_in = n_slices(m + 1);
+    T* ws = t.ws + blockIdx.x * t.ws_stride;
+    double* wsd = t.wsd + blockIdx.x * t.wsd_stride;
+    const T* Fin = t.Fbuf[(m + 1) & 1];
+    const double* fin = t.fbuf[(m + 1) & 1];
+    const T* ain = t.aout[(m + 1) & 1];
     const double* win = t.wout[(m + 1) & 1];
-    double* aout = t.aout[m & 1];
-    double* wout = t.wout[m & 1];
+    const bool from_finest = m == t.M - 2;  // children are finest regions: rows of B^, y~
     for (long loc = blockIdx.x; loc < cnt; loc += gridDim.x) {
         const long i = s0 + loc;
-        if (m == t.M - 2) {
-            // children are finest regions: A_(j,k) = X_j X_k^T over their stacked rows
-            const long cl = t.child_lo[loc], ch = t.child_hi[loc];
-            const long o0 = t.obs_off[cl];
-            const int np = (int)(t.obs_off[ch] - o0);
-            const double* X = t.Bhat + o0 * mr1;  // (L r) x np, ld = L r, L = m+1
-            for (int j = 0; j <= m; ++j)
-                for (int k = j; k <= m; ++k)
-                    gemm<false, true>(r, r, np, 1.0, X + (long)j * r, mr1, X + (long)k * r, mr1, 0.0,
-                                      Aagg + slice_index(m + 1, j, k) * rr, r, sm);
-            gemm<false, false>((int)mr1, 1, np, 1.0, X, mr1, t.yt + o0, np > 0 ? np : 1, 0.0, wagg, mr1, sm);
+        double dterm = 0.0;
+        if (from_finest) {
+            const long lo = t.sub_lo[i];
+            const int n = (int)(t.sub_hi[i] - lo);
+            const T* F = t.Bhat + lo * mr1;
+            const double* f = t.yt + lo;
+            if (t.factored[i]) {
+                T* Fo = m > 0 ? t.Fbuf[m & 1] + lo * (long)m * r : nullptr;
+                double* fo = m > 0 ? t.fbuf[m & 1] + lo : nullptr;
+                factored_step<T>(t, m, i, n, F, mr1, f, Fo, fo, keep != 0, ws, wsd, sm, dterm);
+            } else {
+                T* Aagg = ws;
+                double* wagg = wsd;
+                for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = (T)0;
+                for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = 0.0;
+                __syncthreads();
+                accumulate_factored<T>(t, m, n, F, mr1, f, Aagg, wagg, sm);
+                dense_step<T>(t, m, i, Aagg, wagg, keep != 0, Aagg + ns_in * rr, sm, dterm);
+            }
+        } else if (t.factored[i]) {
+            const long lo = t.sub_lo[i];
+            const int n = (int)(t.sub_hi[i] - lo);
+            T* Fo = m > 0 ? t.Fbuf[m & 1] + lo * (long)m * r : nullptr;
+            double* fo = m > 0 ? t.fbuf[m & 1] + lo : nullptr;
+            factored_step<T>(t, m, i, n, Fin + lo * mr1, mr1, fin + lo, Fo, fo, keep != 0, ws, wsd, sm, dterm);
         } else {
-            const long c0 = i * t.J + 1 - level_start(t.J, m + 1);
-            for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) {
-                double s = 0.0;
-                for (int c = 0; c < t.J; ++c) s += ain[(c0 + c) * ns_in * rr + e];
-                Aagg[e] = s;
-            }
-            for (long e = threadIdx.x; e < mr1; e += kThreads) {
-                double s = 0.0;
-                for (int c = 0; c < t.J; ++c) s += win[(c0 + c) * mr1 + e];
-                wagg[e] = s;
-            }
+            T* Aagg = ws;
+            double* wagg = wsd;
+            for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = (T)0;
+            for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = 0.0;
             __syncthreads();
-        }
-        const double* Lp = t.Lprior + i * rr;
-        double* Lt = t.Lpost + i * rr;
-        double part = 0.0;
-        for (int e = threadIdx.x; e < r; e += kThreads) part -= 2 * log(Lp[e + (long)e * r]);
-        gemm<false, true>(r, r, r, 1.0, Lp, r, Lp, r, 0.0, Lt, r, sm);
-        const double* Amm = Aagg + slice_index(m + 1, m, m) * rr;
-        for (long e = threadIdx.x; e < rr; e += kThreads) Lt[e] += Amm[e];
-        __syncthreads();
-        int info = potrf_lower(r, Lt, r, sm);
-        double* v = t.vpost + i * r;
-        for (int e = threadIdx.x; e < r; e += kThreads) v[e] = wagg[(long)m * r + e];
-        __syncthreads();
-        trsm_left_lower(r, 1, Lt, r, v, r, sm);
-        for (int e = threadIdx.x; e < r; e += kThreads) part += 2 * log(Lt[e + (long)e * r]) - v[e] * v[e];
-        double tot = cta_sum(part, sm);
-        if (threadIdx.x == 0) {
-            t.dpost[i] = tot;
-            if (info) report_error(t.err, i);
-        }
-        if (m > 0) {
-            double* Gi = keep_g ? t.G + t.u_off[m] + loc * (long)m * rr : Gw;  // r x (m r), ld = r
-            for (long e = threadIdx.x; e < (long)m * rr; e += kThreads) {
-                int j = (int)(e / rr);
-                long w = e % rr;
-                int p = (int)(w % r), q = (int)(w / r);
-                Gi[e] = Aagg[slice_index(m + 1, j, m) * rr + q + (long)p * r];  // G_j = A_(j,m)^T
-            }
-            __syncthreads();
-            trsm_left_lower(r, m * r, Lt, r, Gi, r, sm);
-            double* wo = wout + loc * (long)m * r;
-            for (long e = threadIdx.x; e < (long)m * r; e += kThreads) wo[e] = wagg[e];
-            __syncthreads();
-            gemm<true, false>(m * r, 1, r, -1.0, Gi, r, v, r, 1.0, wo, (long)m * r, sm);
-            double* ao = aout + loc * ns_out * rr;
-            for (int j = 0; j < m; ++j) {
-                for (int k = j; k < m; ++k) {
-                    double* dst = ao + slice_index(m, j, k) * rr;
-                    const double* src = Aagg + slice_index(m + 1, j, k) * rr;
-                    for (long e = threadIdx.x; e < rr; e += kThreads) dst[e] = src[e];
+            for (int cc = 1; cc <= t.J; ++cc) {
+                const long c = i * t.J + cc;
+                if (t.factored[c]) {
+                    const long lo = t.sub_lo[c];
+                    accumulate_factored<T>(t, m, (int)(t.sub_hi[c] - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg,
+                                           sm);
+                } else {
+                    const long cl = c - s1;
+                    for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] += ain[cl * ns_in * rr + e];
+                    for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] += win[cl * mr1 + e];
                     __syncthreads();
-                    gemm<true, false>(r, r, r, -1.0, Gi + (long)j * rr, r, Gi + (long)k * rr, r, 1.0, dst, r, sm);
                 }
             }
+            dense_step<T>(t, m, i, Aagg, wagg, keep != 0, Aagg + ns_in * rr, sm, dterm);
         }
+        if (threadIdx.x == 0) t.dpost[i] = dterm;
+        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
 // a12: prediction
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree t) {
-    __shared__ LaSmem sm;
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
+    __shared__ LaSmem<T> sm;
     __shared__ long s_k;
     const int r = t.r, L = t.L;
     const long rr = (long)r * r, Lr = (long)L * r;
@@ -288,71 +474,72 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree t) {
         const long o0 = t.obs_off[k];
         const int n = (int)(t.obs_off[k + 1] - o0);
         const int64_t* anc = t.fin_anc + k * L;
-        double* P = t.P + p0 * Lr;
-        double* Bt = t.Bt + p0 * Lr;
+        T* P = t.P + p0 * Lr;
+        T* Bt = t.Bt + p0 * Lr;
         for (int j = 0; j < L; ++j) {
             const long a = anc[j];
-            double* Cj = Bt + (long)j * r;
-            fill_cov(g, t.pts, a * r, r, t.pred0 + p0, np, false, Cj, Lr);
+            T* Cj = Bt + (long)j * r;
+            fill_cov<T>(g, t.pts, a * r, r, t.pred0 + p0, np, false, Cj, Lr);
             __syncthreads();
             if (j > 0) {
-                const double* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<true, false>(r, np, j * r, -1.0, Ua, (long)j * r, P, Lr, 1.0, Cj, Lr, sm);
+                const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
+                gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, P, Lr, (T)1, Cj, Lr, sm);
             }
-            for (int e = threadIdx.x; e < r * np; e += kThreads) {
-                int tt = e % r, q = e / r;
-                P[(long)j * r + tt + (long)q * Lr] = Cj[tt + (long)q * Lr];
+            for (long e = threadIdx.x; e < (long)r * np; e += kThreads) {
+                int tt = (int)(e % r);
+                long q = e / r;
+                P[(long)j * r + tt + q * Lr] = Cj[tt + q * Lr];
             }
             __syncthreads();
-            trsm_left_lower(r, np, t.Lprior + a * rr, r, P + (long)j * r, Lr, sm);
+            trsm_left_lower<T>(r, np, t.Lprior + a * rr, r, P + (long)j * r, Lr, sm);
         }
         double* mean = t.mean + p0;
         double* var = t.var + p0;
         for (int q = threadIdx.x; q < np; q += kThreads) {
             long ip = t.pred0 + p0 + q;
             double s = t.pts.s2[ip] + t.pts.t2[ip];
-            const double* col = P + (long)q * Lr;
+            const T* col = P + (long)q * Lr;
             double ss = 0.0;
-            for (long x = 0; x < Lr; ++x) ss += col[x] * col[x];
+            for (long x = 0; x < Lr; ++x) ss += (double)col[x] * (double)col[x];
             var[q] = s - ss;
             mean[q] = 0.0;
         }
         __syncthreads();
         if (n > 0) {
-            double* Pc = t.Pc + t.pc_off[k];  // n x np, ld = n
-            fill_cov(g, t.pts, t.obs0 + o0, n, t.pred0 + p0, np, false, Pc, n);
+            T* Pc = t.Pc + t.pc_off[k];  // n x np, ld = n
+            fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.pred0 + p0, np, false, Pc, n);
             __syncthreads();
-            gemm<true, false>(n, np, (int)Lr, -1.0, t.Ufin + o0 * Lr, Lr, P, Lr, 1.0, Pc, n, sm);
-            trsm_left_lower(n, np, t.Lsig + t.lsig_off[k], n, Pc, n, sm);
+            gemm<T, true, false>(n, np, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, P, Lr, (T)1, Pc, n, sm);
+            trsm_left_lower<T>(n, np, t.Lsig + t.lsig_off[k], n, Pc, n, sm);
             const double* yt = t.yt + o0;
             for (int q = threadIdx.x; q < np; q += kThreads) {
-                const double* col = Pc + (long)q * n;
+                const T* col = Pc + (long)q * n;
                 double ss = 0.0, mm = 0.0;
                 for (int x = 0; x < n; ++x) {
-                    ss += col[x] * col[x];
-                    mm += col[x] * yt[x];
+                    ss += (double)col[x] * (double)col[x];
+                    mm += (double)col[x] * yt[x];
                 }
                 var[q] -= ss;
                 mean[q] = mm;
             }
             __syncthreads();
-            gemm<false, false>((int)Lr, np, n, -1.0, t.Bhat + o0 * Lr, Lr, Pc, n, 1.0, Bt, Lr, sm);
+            gemm<T, false, false>((int)Lr, np, n, (T)-1, t.Bhat + o0 * Lr, Lr, Pc, n, (T)1, Bt, Lr, sm);
         }
         for (int j = L - 1; j >= 0; --j) {
             const long a = anc[j];
-            double* KcB = Bt + (long)j * r;
-            trsm_left_lower(r, np, t.Lpost + a * rr, r, KcB, Lr, sm);
+            T* KcB = Bt + (long)j * r;
+            trsm_left_lower<T>(r, np, t.Lpost + a * rr, r, KcB, Lr, sm);
             if (j > 0) {
-                const double* Ga = t.G + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<true, false>(j * r, np, r, -1.0, Ga, r, KcB, Lr, 1.0, Bt, Lr, sm);
+                const T* Ga = t.G + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
+                gemm<T, true, false>(j * r, np, r, (T)-1, Ga, r, KcB, Lr, (T)1, Bt, Lr, sm);
             }
             const double* va = t.vpost + a * r;
             for (int q = threadIdx.x; q < np; q += kThreads) {
-                const double* col = KcB + (long)q * Lr;
+                const T* col = KcB + (long)q * Lr;
                 double ss = 0.0, mm = 0.0;
                 for (int x = 0; x < r; ++x) {
-                    ss += col[x] * col[x];
-                    mm += col[x] * va[x];
+                    ss += (double)col[x] * (double)col[x];
+                    mm += (double)col[x] * va[x];
                 }
                 var[q] += ss;
                 mean[q] += mm;
@@ -363,13 +550,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree t) {
 }
 
 // ---------------------------------------------------------------------------
-// deterministic final sum: d = sum(dfin) + sum(dpost)
+// deterministic final sum: d = sum(dpost) + sum(dfin)
 // ---------------------------------------------------------------------------
-__global__ void k_reduce(DevTree t, double* out) {
-    __shared__ LaSmem sm;
+template <typename T>
+__global__ void k_reduce(DevTree<T> t, double* out) {
+    __shared__ LaSmem<T> sm;
     double s = 0.0;
-    for (long i = threadIdx.x; i < t.n_fin; i += kThreads) s += t.dfin[i];
     for (long i = threadIdx.x; i < t.n_int; i += kThreads) s += t.dpost[i];
+    const long cnt2 = level_count(t.J, t.M - 2);
+    for (long i = threadIdx.x; i < cnt2; i += kThreads) s += t.dfin[i];
     double tot = cta_sum(s, sm);
     if (threadIdx.x == 0) out[0] = tot;
 }
@@ -377,7 +566,8 @@ __global__ void k_reduce(DevTree t, double* out) {
 // ---------------------------------------------------------------------------
 // prior sample y = sum_j U_{obs,j}^T z_{a_j} + L_Sigma z_obs
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_sample(DevTree t, const double* z_int, const double* z_obs,
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 2) k_sample(DevTree<T> t, const double* z_int, const double* z_obs,
                                                     double* y_out) {
     const int r = t.r, L = t.L;
     const long Lr = (long)L * r;
@@ -385,15 +575,15 @@ __global__ void __launch_bounds__(kThreads) k_sample(DevTree t, const double* z_
         const long o0 = t.obs_off[k];
         const int n = (int)(t.obs_off[k + 1] - o0);
         const int64_t* anc = t.fin_anc + k * L;
-        const double* S = t.Lsig + t.lsig_off[k];
+        const T* S = t.Lsig + t.lsig_off[k];
         for (int q = threadIdx.x; q < n; q += kThreads) {
-            const double* col = t.Ufin + (o0 + q) * Lr;
+            const T* col = t.Ufin + (o0 + q) * Lr;
             double y = 0.0;
             for (int j = 0; j < L; ++j) {
                 const double* z = z_int + anc[j] * r;
-                for (int x = 0; x < r; ++x) y += col[(long)j * r + x] * z[x];
+                for (int x = 0; x < r; ++x) y += (double)col[(long)j * r + x] * z[x];
             }
-            for (int x = 0; x <= q; ++x) y += S[q + (long)x * n] * z_obs[o0 + x];
+            for (int x = 0; x <= q; ++x) y += (double)S[q + (long)x * n] * z_obs[o0 + x];
             y_out[o0 + q] = y;
         }
     }
@@ -415,6 +605,12 @@ __global__ void k_cov_block(Geom g, PointSet P, long a0, int na, long b0, int nb
     out[e] = v;
 }
 
+template <typename Ti, typename To>
+__global__ void k_convert(const Ti* __restrict__ in, To* __restrict__ out, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        out[i] = (To)in[i];
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -423,24 +619,33 @@ void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const
     if (n <= 0) return;
     k_fields<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, fp, c0, c1, c2, n, s2, beta, t2);
 }
-void launch_prior_level(const Geom& g, const DevTree& t, int m, int grid, cudaStream_t st) {
+template <typename T>
+void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st) {
     long cnt = level_count(t.J, m);
-    k_prior_level<<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m);
+    k_prior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m);
 }
-void launch_finest(const Geom& g, const DevTree& t, int grid, bool, cudaStream_t st) {
-    k_finest<<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(g, t);
+template <typename T>
+void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
+    long cnt = level_count(t.J, t.M - 2);
+    k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, keep ? 1 : 0);
 }
-void launch_posterior_level(const Geom& g, const DevTree& t, int m, int grid, bool keep_g, cudaStream_t st) {
+template <typename T>
+void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st) {
     long cnt = level_count(t.J, m);
-    k_posterior_level<<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m, keep_g ? 1 : 0);
+    k_posterior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m, keep ? 1 : 0);
 }
-void launch_predict(const Geom& g, const DevTree& t, int grid, cudaStream_t st) {
-    k_predict<<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(g, t);
+template <typename T>
+void launch_predict(const Geom& g, const DevTree<T>& t, int grid, cudaStream_t st) {
+    k_predict<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(g, t);
 }
-void launch_reduce(const DevTree& t, double* out, cudaStream_t st) { k_reduce<<<1, kThreads, 0, st>>>(t, out); }
-void launch_sample(const DevTree& t, const double* z_int, const double* z_obs, double* y_out, int grid,
+template <typename T>
+void launch_reduce(const DevTree<T>& t, double* out, cudaStream_t st) {
+    k_reduce<T><<<1, kThreads, 0, st>>>(t, out);
+}
+template <typename T>
+void launch_sample(const DevTree<T>& t, const double* z_int, const double* z_obs, double* y_out, int grid,
                    cudaStream_t st) {
-    k_sample<<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(t, z_int, z_obs, y_out);
+    k_sample<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(t, z_int, z_obs, y_out);
 }
 void launch_cov_block(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self, double* out,
                       cudaStream_t st) {
@@ -448,5 +653,24 @@ void launch_cov_block(const Geom& g, const PointSet& P, long a0, int na, long b0
     if (n <= 0) return;
     k_cov_block<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, P, a0, na, b0, nb, self ? 1 : 0, out);
 }
+
+template <typename Ti, typename To>
+void launch_convert(const Ti* in, To* out, long n, cudaStream_t st) {
+    if (n <= 0) return;
+    long blocks = (n + 255) / 256;
+    k_convert<Ti, To><<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(in, out, n);
+}
+template void launch_convert<float, double>(const float*, double*, long, cudaStream_t);
+template void launch_convert<double, float>(const double*, float*, long, cudaStream_t);
+
+#define MRA_INSTANTIATE(T)                                                                                   \
+    template void launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t);            \
+    template void launch_finest_group<T>(const Geom&, const DevTree<T>&, int, bool, cudaStream_t);          \
+    template void launch_posterior_level<T>(const Geom&, const DevTree<T>&, int, int, bool, cudaStream_t);  \
+    template void launch_predict<T>(const Geom&, const DevTree<T>&, int, cudaStream_t);                     \
+    template void launch_reduce<T>(const DevTree<T>&, double*, cudaStream_t);                               \
+    template void launch_sample<T>(const DevTree<T>&, const double*, const double*, double*, int, cudaStream_t);
+MRA_INSTANTIATE(double)
+MRA_INSTANTIATE(float)
 
 }  // namespace mra

@@ -1,5 +1,6 @@
-// Launch interface between the C-ABI layer (mra_api.cu) and the FP64 region
-// kernels (mra_kernels.cu).
+// Launch interface between the C-ABI layer (mra_api.cu) and the region
+// kernels (mra_kernels.cu), templated on the storage type T (double: plain
+// FP64 path, float: mixed path).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,42 +11,54 @@
 namespace mra {
 
 // Everything a kernel needs to address the resident structure and buffers.
+template <typename T>
 struct DevTree {
     int J, M, r, L;            // L = M-1 ancestor levels of a finest region
     long n_int, n_fin, n_obs, n_pred;
     long obs0, pred0;          // first obs / pred index in the joint point arrays
-    PointSet pts;              // knots | obs | preds, with their fields
+    int tf;                    // largest subtree (in observations) kept in factored form
+    PointSet pts;              // knots | obs | preds, with their fields (FP64)
     const double* y;           // [n_obs]
     const int64_t* obs_off;    // [n_fin+1]
-    const int64_t* pred_off;   // [n_fin+1] (or nullptr)
+    const int64_t* pred_off;   // [n_fin+1]
     const int64_t* fin_anc;    // [n_fin][L] ancestors of each finest region, level 0 first
-    const int64_t* fin_order;  // [n_fin] finest regions, most expensive first
-    const int64_t* lsig_off;   // [n_fin+1] offsets of the n_k x n_k blocks
-    const int64_t* pc_off;     // [n_fin+1] offsets of the n_k x n_p,k prediction blocks
+    const int64_t* sub_lo;     // [n_int] first observation of each interior region's subtree
+    const int64_t* sub_hi;     // [n_int] one past the last
     const int64_t* child_lo;   // [J^(M-2)] first finest child of each level M-2 region
     const int64_t* child_hi;   // one past the last
-    int64_t u_off[kMaxLevels]; // offset of level m's U (= G) blocks, m*r*r doubles per region
+    const int64_t* par_order;  // [J^(M-2)] level M-2 regions (local index), most expensive first
+    const int64_t* fin_order;  // [n_fin] finest regions, most expensive prediction work first
+    const int8_t* factored;    // [n_int] 1: the region's posterior output is kept as F, f
+    const int64_t* lsig_off;   // [n_fin+1] offsets of the n_k x n_k blocks
+    const int64_t* pc_off;     // [n_fin+1] offsets of the n_k x n_p,k prediction blocks
+    int64_t u_off[kMaxLevels]; // offset of level m's U (= G) blocks, m*r*r per region
     // prior
-    double* Lprior;            // [n_int][r*r]
-    double* U;                 // per level m: [J^m][(m r) x r], ld = m r
-    double* Ufin;              // [n_obs][L r]   finest U_{k,j} columns, obs-major
-    double* Bhat;              // [n_obs][L r]   B^_k transposed, obs-major
-    double* yt;                // [n_obs]        L_Sigma^{-1} y per region
-    double* Lsig;              // CSR n_k x n_k  finest Cholesky factors
-    double* dfin;              // [n_fin]
+    T* Lprior;                 // [n_int][r*r]
+    double* ldprior;           // [n_int] 2 sum log diag of the prior factor
+    T* U;                      // per level m: [J^m][(m r) x r], ld = m r
+    T* Ufin;                   // [n_obs][L r]   finest U_{k,j} columns, obs-major
+    T* Bhat;                   // [n_obs][L r]   B^ transposed, obs-major (the finest F)
+    double* yt;                // [n_obs]        L_Sigma^{-1} y (the finest f)
+    T* Lsig;                   // CSR n_k x n_k  finest Cholesky factors
     // posterior
-    double* Lpost;             // [n_int][r*r]
+    T* Lpost;                  // [n_int][r*r]
     double* vpost;             // [n_int][r]
-    double* G;                 // same layout as U: [J^m][r x (m r)], ld = r
-    double* dpost;             // [n_int]
-    double* aout[2];           // ping-pong A~ slices of one level
-    double* wout[2];           // ping-pong w~ of one level
-    double* ws;                // per-CTA posterior workspace
-    long ws_stride;            // doubles per CTA
+    T* G;                      // like U: [J^m][r x (m r)], ld = r (prediction mode)
+    double* dpost;             // [n_int] posterior log-lik terms
+    double* dfin;              // [J^(M-2)] finest-level log-lik terms of each sibling group
+    int fuse_post;             // 1: the finest-group kernel also runs the level M-2 posterior
+    T* aout[2];                // dense A~ slices of one level, ping-pong by level parity
+    double* wout[2];           // dense w~ of one level
+    T* Fbuf[2];                // factored F of one level: [n_obs][m r]
+    double* fbuf[2];           // factored f of one level: [n_obs]
+    T* ws;                     // per-CTA workspace (T)
+    long ws_stride;
+    double* wsd;               // per-CTA workspace (FP64)
+    long wsd_stride;
     // prediction
-    double* P;                 // [n_pred][L r]
-    double* Bt;                // [n_pred][L r]
-    double* Pc;                // CSR n_k x n_p,k
+    T* P;                      // [n_pred][L r]
+    T* Bt;                     // [n_pred][L r]
+    T* Pc;                     // CSR n_k x n_p,k
     double* mean;              // [n_pred]
     double* var;               // [n_pred]
     // bookkeeping
@@ -83,12 +96,21 @@ void set_last_error(const char* msg);
 
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
-void launch_prior_level(const Geom& g, const DevTree& t, int m, int grid, cudaStream_t st);
-void launch_finest(const Geom& g, const DevTree& t, int grid, bool keep_ufin, cudaStream_t st);
-void launch_posterior_level(const Geom& g, const DevTree& t, int m, int grid, bool keep_g, cudaStream_t st);
-void launch_predict(const Geom& g, const DevTree& t, int grid, cudaStream_t st);
-void launch_reduce(const DevTree& t, double* out, cudaStream_t st);
-void launch_sample(const DevTree& t, const double* z_int, const double* z_obs, double* y_out, int grid,
+template <typename T>
+void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st);
+template <typename T>
+void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st);
+template <typename T>
+void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st);
+template <typename T>
+void launch_predict(const Geom& g, const DevTree<T>& t, int grid, cudaStream_t st);
+template <typename T>
+void launch_reduce(const DevTree<T>& t, double* out, cudaStream_t st);
+// out[i] = (To) in[i]
+template <typename Ti, typename To>
+void launch_convert(const Ti* in, To* out, long n, cudaStream_t st);
+template <typename T>
+void launch_sample(const DevTree<T>& t, const double* z_int, const double* z_obs, double* y_out, int grid,
                    cudaStream_t st);
 void launch_cov_block(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self, double* out,
                       cudaStream_t st);

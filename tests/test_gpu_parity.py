@@ -198,3 +198,32 @@ def test_bad_theta_rejected():
         ctx.set_theta(sill_scale=float("nan"))
     assert e.value.status == capi.MRA_ERR_ARG
     ctx.close()
+
+
+# ---------------------------------------------------------------------------
+# mixed path: FP32 tensor-core prior and finest level, FP64 posterior
+# ---------------------------------------------------------------------------
+MIXED_LL_RTOL = 1e-6
+
+
+def test_mixed_golden_loglik(case_dir):
+    g = json.load(open(os.path.join(case_dir, "golden.json")))
+    st, md, _ = refio.load_case(case_dir, mode="likelihood")
+    ctx, (d, ll) = run_loglik(st, md, precision="mixed")
+    err = abs(ll - g["loglik"]) / abs(g["loglik"])
+    print(f"mixed loglik rel err {os.path.basename(case_dir)}: {err:.3e}")
+    assert err <= MIXED_LL_RTOL, (ll, g["loglik"], err)
+    ctx.close()
+
+
+def test_mixed_golden_predict_error_report(case_dir):
+    st, md, _ = refio.load_case(case_dir, mode="prediction")
+    lon, lat, mean, var = refio.read_prediction_dump(os.path.join(case_dir, "pred_golden.bin"))
+    ctx = api.Context(st, md, precision="mixed")
+    ctx.set_theta(**theta_of(md))
+    m, v = ctx.predict()
+    em = np.max(np.abs(m - mean) / np.maximum(1.0, np.abs(mean)))
+    ev = np.max(np.abs(v - var) / np.maximum(1.0, np.abs(var)))
+    print(f"mixed prediction err {os.path.basename(case_dir)}: mean {em:.3e} var {ev:.3e}")
+    assert em <= 1e-4 and ev <= 1e-4
+    ctx.close()
