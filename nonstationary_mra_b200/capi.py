@@ -58,11 +58,23 @@ class mra_stats(C.Structure):
                 ("n_timed", C.c_int32), ("timed_kind", C.c_int32 * 40), ("timed_level", C.c_int32 * 40),
                 ("timed_ms", C.c_double * 40), ("timed_flop", C.c_double * 40)]
 
+class mra_opt_config(C.Structure):
+    _fields_ = [("rho_begin", C.c_double), ("rho_end", C.c_double), ("npt", C.c_int32), ("max_evals", C.c_int32)]
+
+
+class mra_opt_result(C.Structure):
+    _fields_ = [("f_best", C.c_double), ("evals", C.c_int32), ("status", C.c_int32), ("rho_final", C.c_double)]
+
+
+# double (*)(const double* x, void* user, int32_t* stop)
+OBJECTIVE_FN = C.CFUNCTYPE(C.c_double, _p_f64, C.c_void_p, C.POINTER(C.c_int32))
+_p_f32 = C.POINTER(C.c_float)
+
 KERNEL_NAMES = {0: "fields", 1: "prior_level", 2: "finest_group", 3: "posterior_level", 4: "reduce", 5: "predict",
                 6: "convert"}
 
 
-# (name, restype, argtypes) of every exported entry point of include/mra_b200.h
+# (name, restype, argtypes) of every exported entry point of include/mra_b200.h and include/mra_surrogate.h
 SIGNATURES = [
     ("mra_create", C.c_int, [C.POINTER(mra_structure), C.POINTER(mra_model), C.c_int32, C.POINTER(C.c_void_p)]),
     ("mra_destroy", C.c_int, [C.c_void_p]),
@@ -82,6 +94,18 @@ SIGNATURES = [
     ("mra_timer_start", C.c_int, [C.c_void_p]),
     ("mra_timer_stop", C.c_int, [C.c_void_p, _p_f64]),
     ("mra_last_error", C.c_char_p, []),
+    # include/mra_surrogate.h
+    ("mra_opt_minimize", C.c_int, [C.c_int32, _p_f64, _p_f64, _p_f64, C.POINTER(mra_opt_config), OBJECTIVE_FN,
+                                   C.c_void_p, C.POINTER(mra_opt_result)]),
+    ("mra_mlp_create", C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("mra_mlp_destroy", C.c_int, [C.c_void_p]),
+    ("mra_mlp_num_params", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("mra_mlp_get_params", C.c_int, [C.c_void_p, _p_f32]),
+    ("mra_mlp_set_params", C.c_int, [C.c_void_p, _p_f32]),
+    ("mra_mlp_set_data", C.c_int, [C.c_void_p, _p_f32, _p_f32, C.c_int64]),
+    ("mra_mlp_grad", C.c_int, [C.c_void_p, _p_f32, _p_f32]),
+    ("mra_mlp_train", C.c_int, [C.c_void_p, C.c_int32, C.c_float, _p_f32]),
+    ("mra_mlp_predict", C.c_int, [C.c_void_p, _p_f32, C.c_int64, _p_f32, _p_f32]),
 ]
 
 _lib: Optional[C.CDLL] = None
@@ -121,3 +145,7 @@ def f64p(a: np.ndarray):
 
 def u64p(a: np.ndarray):
     return a.ctypes.data_as(_p_u64)
+
+
+def f32p(a: np.ndarray):
+    return a.ctypes.data_as(_p_f32)

@@ -526,6 +526,8 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     c->geom = make_geom(m);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(MRA_ERR_CUDA, "stream creation failed"));
+    if (cudaError_t pe = prepare_kernels(); pe != cudaSuccess)
+        return bail(fail(MRA_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(pe)));
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "event creation failed"));
     for (auto& e : c->tev)

@@ -160,11 +160,22 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 // ----------------------------------------------------------------------------
 constexpr int TM = 64, TN = 64, TK = 16, NB = 16;
 
+// FP64 products (T = double): CTA tile 64 x (16 NW), NW in {1, 2, 4} picked by
+// the width of the product, K slabs of 32.  Each operand tile is staged in
+// shared memory in the layout of its global storage -- K-contiguous operands
+// as [row][k] (stride 36), the others as [k][row] (stride 68) -- so that the
+// coalesced global reads, the staging stores and the m8n8k4 fragment loads
+// are all free of bank conflicts (both strides are 4 mod 16 doubles).
+constexpr int TK64 = 32;
+constexpr int KS64 = TK64 + 4;
+constexpr int RS64 = 64 + 4;
+constexpr int TILE64 = 64 * KS64;  // >= TK64 * RS64
+
 template <typename T>
 struct TilePad;
 template <>
 struct TilePad<double> {
-    static constexpr int v = 4;  // row stride 68 doubles: conflict-free m8n8k4 fragment loads
+    static constexpr int v = 4;
 };
 template <>
 struct TilePad<float> {
@@ -172,59 +183,160 @@ struct TilePad<float> {
 };
 
 template <typename T>
-struct LaSmem {
-    T A[TK][TM + TilePad<T>::v];
-    T B[TK][TN + TilePad<T>::v];
+struct LaSmem;
+template <>
+struct LaSmem<double> {
+    double A[2][TILE64];   // two pipeline stages of each operand tile
+    double B[2][TILE64];
+    double D[NB][NB + 1];  // staged diagonal block
+    double inv[NB];        // reciprocals of its diagonal
+    double red[kThreads / 32];
+    int flag;
+};
+template <>
+struct LaSmem<float> {
+    float A[TK][TM + TilePad<float>::v];
+    float B[TK][TN + TilePad<float>::v];
     double D[NB][NB + 1];  // staged diagonal block (always FP64)
+    double inv[NB];
     double red[kThreads / 32];
     int flag;
 };
 
-// Warp tile: 32 rows x 16 columns of the 64 x 64 CTA tile.
+// The region kernels keep their LaSmem in dynamic shared memory (the FP64
+// version is larger than the 48 KB static limit).
 template <typename T>
-struct Acc;
-template <>
-struct Acc<double> {
-    double v[4][2][2];  // 4 (m8) x 2 (n8) fragments of m8n8
-};
-template <>
-struct Acc<float> {
-    float v[2][2][4];  // 2 (m16) x 2 (n8) fragments of m16n8
-};
-
-__device__ __forceinline__ void acc_zero(Acc<double>& a) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) a.v[i][j][0] = a.v[i][j][1] = 0.0;
-}
-__device__ __forceinline__ void acc_zero(Acc<float>& a) {
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) a.v[i][j][q] = 0.f;
+__device__ __forceinline__ LaSmem<T>& la_smem() {
+    extern __shared__ __align__(16) unsigned char la_dyn_smem[];
+    return *reinterpret_cast<LaSmem<T>*>(la_dyn_smem);
 }
 
-// one TK-deep step of the warp tile from the staged tiles
-__device__ __forceinline__ void warp_step(Acc<double>& acc, const LaSmem<double>& sm, int wm, int wn, int lane) {
+// ---- FP64: warp tile (8 NW) rows x 16 columns --------------------------------
+template <int NW>
+struct AccD {
+    double v[NW][2][2];  // NW (m8) x 2 (n8) fragments of m8n8
+};
+
+// 8-byte asynchronous global -> shared copy; pred == false writes zeros.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool pred) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <bool TA, bool TB, int NW>
+__device__ __forceinline__ void warp_step_f64(AccD<NW>& acc, const double* sA, const double* sB, int wm, int wn,
+                                              int lane) {
     const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-    for (int k4 = 0; k4 < TK; k4 += 4) {
-        double a[4], b[2];
+    for (int k4 = 0; k4 < TK64; k4 += 4) {
+        double a[NW], b[2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = sm.A[k4 + t][wm + 8 * i + g];
+        for (int i = 0; i < NW; ++i) {
+            const int row = wm + 8 * i + g, k = k4 + t;
+            a[i] = TA ? sA[row * KS64 + k] : sA[k * RS64 + row];
+        }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) b[j] = sm.B[k4 + t][wn + 8 * j + g];
+        for (int j = 0; j < 2; ++j) {
+            const int col = wn + 8 * j + g, k = k4 + t;
+            b[j] = TB ? sB[k * RS64 + col] : sB[col * KS64 + k];
+        }
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < NW; ++i)
 #pragma unroll
             for (int j = 0; j < 2; ++j) mma_f64(acc.v[i][j], a[i], b[j]);
     }
 }
 
-__device__ __forceinline__ void warp_step(Acc<float>& acc, const LaSmem<float>& sm, int wm, int wn, int lane) {
+// Operands must be in global memory (they are copied with cp.async): a
+// two-stage pipeline keeps the next K slab in flight while the tensor pipe
+// works on the current one.
+template <bool TA, bool TB, int NW>
+__device__ inline void gemm_f64(int M, int N, int K, double alpha, const double* A, long lda, const double* B,
+                                long ldb, double beta, double* C, long ldc, LaSmem<double>& sm) {
+    constexpr int W = 16 * NW;                // CTA tile width
+    constexpr int WM = 8 / NW;                // warps along M
+    constexpr int PA = 64 * TK64 / kThreads;  // A elements per thread per slab (8)
+    constexpr int PB = W * TK64 / kThreads;   // B elements per thread per slab (2 NW)
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int wm = (w % WM) * 8 * NW, wn = (w / WM) * 16;
+    for (int m0 = 0; m0 < M; m0 += 64) {
+        for (int n0 = 0; n0 < N; n0 += W) {
+            AccD<NW> acc;
+#pragma unroll
+            for (int i = 0; i < NW; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) acc.v[i][j][0] = acc.v[i][j][1] = 0.0;
+            auto issue = [&](int k0, int stage) {
+                double* sA = sm.A[stage];
+                double* sB = sm.B[stage];
+#pragma unroll
+                for (int q = 0; q < PA; ++q) {
+                    const int e = tid + q * kThreads;
+                    // TA: op(A)[i][k] = A[k + i lda] (K-contiguous), else A[i + k lda]
+                    const int i = TA ? e / TK64 : e % 64, k = TA ? e % TK64 : e / 64;
+                    const int gi = m0 + i, gk = k0 + k;
+                    const bool ok = gi < M && gk < K;
+                    const double* src = ok ? (TA ? A + gk + (long)gi * lda : A + gi + (long)gk * lda) : A;
+                    cp_async8(sA + (TA ? i * KS64 + k : k * RS64 + i), src, ok);
+                }
+#pragma unroll
+                for (int q = 0; q < PB; ++q) {
+                    const int e = tid + q * kThreads;
+                    // TB: op(B)[k][j] = B[j + k ldb], else B[k + j ldb] (K-contiguous)
+                    const int j = TB ? e % W : e / TK64, k = TB ? e / W : e % TK64;
+                    const int gj = n0 + j, gk = k0 + k;
+                    const bool ok = gj < N && gk < K;
+                    const double* src = ok ? (TB ? B + gj + (long)gk * ldb : B + gk + (long)gj * ldb) : B;
+                    cp_async8(sB + (TB ? k * RS64 + j : j * KS64 + k), src, ok);
+                }
+                cp_async_commit();
+            };
+            // warps whose tile lies outside the product skip the tensor work
+            const bool active = m0 + wm < M && n0 + wn < N;
+            if (K > 0) issue(0, 0);
+            int stage = 0;
+            for (int k0 = 0; k0 < K; k0 += TK64, stage ^= 1) {
+                if (k0 + TK64 < K) {
+                    issue(k0 + TK64, stage ^ 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                if (active) warp_step_f64<TA, TB, NW>(acc, sm.A[stage], sm.B[stage], wm, wn, lane);
+                __syncthreads();
+            }
+            if (active) {
+                const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+                for (int i = 0; i < NW; ++i)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) {
+                        const int r = m0 + wm + 8 * i + g, c = n0 + wn + 8 * j + 2 * t;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            if (r < M && c + h < N) {
+                                double* p = C + r + (long)(c + h) * ldc;
+                                *p = beta == 0.0 ? alpha * acc.v[i][j][h] : alpha * acc.v[i][j][h] + beta * *p;
+                            }
+                        }
+                    }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---- FP32 storage (mixed path): 3xTF32 products, 64 x 64 tiles, K slabs of 16
+struct AccF {
+    float v[2][2][4];  // 2 (m16) x 2 (n8) fragments of m16n8
+};
+
+__device__ __forceinline__ void warp_step_tf32x3(AccF& acc, const LaSmem<float>& sm, int wm, int wn, int lane) {
     const int g = lane >> 2, t = lane & 3;
 #pragma unroll
     for (int k8 = 0; k8 < TK; k8 += 8) {
@@ -260,56 +372,22 @@ __device__ __forceinline__ void warp_step(Acc<float>& acc, const LaSmem<float>& 
     }
 }
 
-// write back: C = alpha*acc + beta*C for the warp tile
-template <typename T>
-__device__ __forceinline__ void put(T* C, long ldc, int M, int N, int r, int c, T alpha, T beta, T v) {
-    if (r < M && c < N) {
-        T* p = C + r + (long)c * ldc;
-        *p = beta == (T)0 ? alpha * v : alpha * v + beta * *p;
-    }
-}
-__device__ __forceinline__ void acc_store(const Acc<double>& acc, double* C, long ldc, int M, int N, int m0, int n0,
-                                          int wm, int wn, int lane, double alpha, double beta) {
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int r = m0 + wm + 8 * i + g, c = n0 + wn + 8 * j + 2 * t;
-            put(C, ldc, M, N, r, c, alpha, beta, acc.v[i][j][0]);
-            put(C, ldc, M, N, r, c + 1, alpha, beta, acc.v[i][j][1]);
-        }
-}
-__device__ __forceinline__ void acc_store(const Acc<float>& acc, float* C, long ldc, int M, int N, int m0, int n0,
-                                          int wm, int wn, int lane, float alpha, float beta) {
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * t;
-            put(C, ldc, M, N, r, c, alpha, beta, acc.v[i][j][0]);
-            put(C, ldc, M, N, r, c + 1, alpha, beta, acc.v[i][j][1]);
-            put(C, ldc, M, N, r + 8, c, alpha, beta, acc.v[i][j][2]);
-            put(C, ldc, M, N, r + 8, c + 1, alpha, beta, acc.v[i][j][3]);
-        }
-}
-
-// C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N, column-major,
-// any leading dimensions, global or shared memory.  beta == 0 never reads C.
-// The next TK-deep slab is fetched into registers while the tensor pipe works
-// on the current one.  Ends with a barrier.
-template <typename T, bool TA, bool TB>
-__device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta, T* C,
-                            long ldc, LaSmem<T>& sm) {
+template <bool TA, bool TB>
+__device__ inline void gemm_f32(int M, int N, int K, float alpha, const float* A, long lda, const float* B, long ldb,
+                                float beta, float* C, long ldc, LaSmem<float>& sm) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
     constexpr int PER = TK * TM / kThreads;  // elements of each operand per thread per slab (4)
     for (int m0 = 0; m0 < M; m0 += TM) {
         for (int n0 = 0; n0 < N; n0 += TN) {
-            Acc<T> acc;
-            acc_zero(acc);
-            T ra[PER], rb[PER];
+            AccF acc;
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc.v[i][j][q] = 0.f;
+            float ra[PER], rb[PER];
             auto fetch = [&](int k0) {
 #pragma unroll
                 for (int q = 0; q < PER; ++q) {
@@ -317,11 +395,11 @@ __device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, 
                     int i, k;
                     if (!TA) { i = e % TM; k = e / TM; } else { k = e % TK; i = e / TK; }
                     const int gi = m0 + i, gk = k0 + k;
-                    ra[q] = (gi < M && gk < K) ? (TA ? A[gk + (long)gi * lda] : A[gi + (long)gk * lda]) : (T)0;
+                    ra[q] = (gi < M && gk < K) ? (TA ? A[gk + (long)gi * lda] : A[gi + (long)gk * lda]) : 0.f;
                     int j, kb;
                     if (!TB) { kb = e % TK; j = e / TK; } else { j = e % TN; kb = e / TN; }
                     const int gj = n0 + j, gkb = k0 + kb;
-                    rb[q] = (gj < N && gkb < K) ? (TB ? B[gj + (long)gkb * ldb] : B[gkb + (long)gj * ldb]) : (T)0;
+                    rb[q] = (gj < N && gkb < K) ? (TB ? B[gj + (long)gkb * ldb] : B[gkb + (long)gj * ldb]) : 0.f;
                 }
             };
             auto stash = [&]() {
@@ -344,16 +422,58 @@ __device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, 
             for (int k0 = 0; k0 < K; k0 += TK) {
                 const bool more = k0 + TK < K;
                 if (more) fetch(k0 + TK);
-                warp_step(acc, sm, wm, wn, lane);
+                warp_step_tf32x3(acc, sm, wm, wn, lane);
                 __syncthreads();
                 if (more) {
                     stash();
                     __syncthreads();
                 }
             }
-            acc_store(acc, C, ldc, M, N, m0, n0, wm, wn, lane, alpha, beta);
+            const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * t;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int rr = r + (q >> 1) * 8, cc = c + (q & 1);
+                        if (rr < M && cc < N) {
+                            float* p = C + rr + (long)cc * ldc;
+                            *p = beta == 0.f ? alpha * acc.v[i][j][q] : alpha * acc.v[i][j][q] + beta * *p;
+                        }
+                    }
+                }
         }
     }
+    __syncthreads();
+}
+
+// C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N, column-major,
+// any leading dimensions; A and B in global memory.  beta == 0 never reads C.
+// Ends with a barrier.
+template <typename T, bool TA, bool TB>
+__device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta, T* C,
+                            long ldc, LaSmem<T>& sm) {
+    if constexpr (sizeof(T) == 8) {
+        if (N <= 16) gemm_f64<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        else if (N <= 32) gemm_f64<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        else gemm_f64<TA, TB, 4>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+    } else {
+        gemm_f32<TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+    }
+}
+
+// Stages the nb x nb diagonal block of L at b0 in FP64 with the reciprocals of
+// its diagonal.  Ends with a barrier.
+template <typename T>
+__device__ inline void stage_diag_block(const T* L, long ldl, int b0, int nb, LaSmem<T>& sm) {
+    for (int e = threadIdx.x; e < nb * nb; e += kThreads) {
+        int i = e % nb, j = e / nb;
+        sm.D[i][j] = (double)L[(b0 + i) + (long)(b0 + j) * ldl];
+    }
+    __syncthreads();
+    if (threadIdx.x < nb) sm.inv[threadIdx.x] = 1.0 / sm.D[threadIdx.x][threadIdx.x];
     __syncthreads();
 }
 
@@ -364,11 +484,7 @@ __device__ inline void trsm_left_lower(int n, int nrhs, const T* L, long ldl, T*
     const int tid = threadIdx.x;
     for (int b0 = 0; b0 < n; b0 += NB) {
         int nb = min(NB, n - b0);
-        for (int e = tid; e < nb * nb; e += kThreads) {
-            int i = e % nb, j = e / nb;
-            sm.D[i][j] = (double)L[(b0 + i) + (long)(b0 + j) * ldl];
-        }
-        __syncthreads();
+        stage_diag_block(L, ldl, b0, nb, sm);
         for (int c = tid; c < nrhs; c += kThreads) {
             double x[NB];
             T* col = B + b0 + (long)c * ldb;
@@ -380,7 +496,7 @@ __device__ inline void trsm_left_lower(int n, int nrhs, const T* L, long ldl, T*
                     double s = x[i];
 #pragma unroll
                     for (int k = 0; k < i; ++k) s -= sm.D[i][k] * x[k];
-                    x[i] = s / sm.D[i][i];
+                    x[i] = s * sm.inv[i];
                 }
             }
 #pragma unroll
@@ -400,11 +516,7 @@ __device__ inline void trsm_right_lower_trans(int rows, int n, const T* L, long 
     const int tid = threadIdx.x;
     for (int b0 = 0; b0 < n; b0 += NB) {
         int nb = min(NB, n - b0);
-        for (int e = tid; e < nb * nb; e += kThreads) {
-            int i = e % nb, j = e / nb;
-            sm.D[i][j] = (double)L[(b0 + i) + (long)(b0 + j) * ldl];
-        }
-        __syncthreads();
+        stage_diag_block(L, ldl, b0, nb, sm);
         for (int row = tid; row < rows; row += kThreads) {
             double x[NB];
             T* p = B + row + (long)b0 * ldb;
@@ -416,7 +528,7 @@ __device__ inline void trsm_right_lower_trans(int rows, int n, const T* L, long 
                     double s = x[i];
 #pragma unroll
                     for (int k = 0; k < i; ++k) s -= sm.D[i][k] * x[k];
-                    x[i] = s / sm.D[i][i];
+                    x[i] = s * sm.inv[i];
                 }
             }
 #pragma unroll
@@ -465,24 +577,30 @@ __device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* 
             sm.D[i][j] = (double)A[(b0 + i) + (long)(b0 + j) * lda];
         }
         __syncthreads();
-        for (int k = 0; k < nb; ++k) {
-            if (tid == 0) {
-                double d = sm.D[k][k];
-                if (!(d > 0.0) && sm.flag == 0) sm.flag = b0 + k + 1;
-                sm.D[k][k] = sqrt(d);
-                ld += 2.0 * log(sm.D[k][k]);
+        // the diagonal block by warp 0, lane i owning row i (right-looking)
+        if (tid < 32) {
+            const int lane = tid;
+            for (int k = 0; k < nb; ++k) {
+                if (lane == 0) {
+                    double d = sm.D[k][k];
+                    if (!(d > 0.0) && sm.flag == 0) sm.flag = b0 + k + 1;
+                    double sq = sqrt(d);
+                    sm.D[k][k] = sq;
+                    sm.inv[k] = 1.0 / sq;
+                    ld += 2.0 * log(sq);
+                }
+                __syncwarp();
+                if (lane > k && lane < nb) sm.D[lane][k] *= sm.inv[k];
+                __syncwarp();
+                // lane i reads column k (final) and writes row i beyond column k
+                if (lane > k && lane < nb) {
+                    const double lik = sm.D[lane][k];
+                    for (int j = k + 1; j <= lane; ++j) sm.D[lane][j] -= lik * sm.D[j][k];
+                }
+                __syncwarp();
             }
-            __syncthreads();
-            double dk = sm.D[k][k];
-            for (int i = k + 1 + tid; i < nb; i += kThreads) sm.D[i][k] /= dk;
-            __syncthreads();
-            int rem = nb - k - 1;
-            for (int e = tid; e < rem * rem; e += kThreads) {
-                int i = k + 1 + e % rem, j = k + 1 + e / rem;
-                if (j <= i) sm.D[i][j] -= sm.D[i][k] * sm.D[j][k];
-            }
-            __syncthreads();
         }
+        __syncthreads();
         for (int e = tid; e < nb * nb; e += kThreads) {
             int i = e % nb, j = e / nb;
             A[(b0 + i) + (long)(b0 + j) * lda] = j <= i ? (T)sm.D[i][j] : (T)0;
@@ -502,7 +620,7 @@ __device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* 
                         double s = x[i];
 #pragma unroll
                         for (int k = 0; k < i; ++k) s -= sm.D[i][k] * x[k];
-                        x[i] = s / sm.D[i][i];
+                        x[i] = s * sm.inv[i];
                     }
                 }
 #pragma unroll

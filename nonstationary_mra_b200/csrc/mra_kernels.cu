@@ -90,7 +90,7 @@ __global__ void k_fields(Geom g, FieldParams fp, const double* __restrict__ c0, 
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> t, int m) {
-    __shared__ LaSmem<T> sm;
+    LaSmem<T>& sm = la_smem<T>();
     const int r = t.r;
     const long rr = (long)r * r;
     const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
@@ -280,7 +280,7 @@ __device__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* 
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T> t, int keep) {
-    __shared__ LaSmem<T> sm;
+    LaSmem<T>& sm = la_smem<T>();
     __shared__ long s_p;
     const int r = t.r, L = t.L, m = t.M - 2;
     const long rr = (long)r * r, Lr = (long)L * r;
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree<T> t, int m, int keep) {
-    __shared__ LaSmem<T> sm;
+    LaSmem<T>& sm = la_smem<T>();
     const int r = t.r;
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
     const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
-    __shared__ LaSmem<T> sm;
+    LaSmem<T>& sm = la_smem<T>();
     __shared__ long s_k;
     const int r = t.r, L = t.L;
     const long rr = (long)r * r, Lr = (long)L * r;
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_reduce(DevTree<T> t, double* out) {
-    __shared__ LaSmem<T> sm;
+    LaSmem<T>& sm = la_smem<T>();
     double s = 0.0;
     for (long i = threadIdx.x; i < t.n_int; i += kThreads) s += t.dpost[i];
     const long cnt2 = level_count(t.J, t.M - 2);
@@ -622,30 +622,30 @@ void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const
 template <typename T>
 void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st) {
     long cnt = level_count(t.J, m);
-    k_prior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m);
+    k_prior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, m);
 }
 template <typename T>
 void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
     long cnt = level_count(t.J, t.M - 2);
-    k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, keep ? 1 : 0);
+    k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, keep ? 1 : 0);
 }
 template <typename T>
 void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st) {
     long cnt = level_count(t.J, m);
-    k_posterior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, 0, st>>>(g, t, m, keep ? 1 : 0);
+    k_posterior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, m, keep ? 1 : 0);
 }
 template <typename T>
 void launch_predict(const Geom& g, const DevTree<T>& t, int grid, cudaStream_t st) {
-    k_predict<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(g, t);
+    k_predict<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t);
 }
 template <typename T>
 void launch_reduce(const DevTree<T>& t, double* out, cudaStream_t st) {
-    k_reduce<T><<<1, kThreads, 0, st>>>(t, out);
+    k_reduce<T><<<1, kThreads, sizeof(LaSmem<T>), st>>>(t, out);
 }
 template <typename T>
 void launch_sample(const DevTree<T>& t, const double* z_int, const double* z_obs, double* y_out, int grid,
                    cudaStream_t st) {
-    k_sample<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, 0, st>>>(t, z_int, z_obs, y_out);
+    k_sample<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, sizeof(LaSmem<T>), st>>>(t, z_int, z_obs, y_out);
 }
 void launch_cov_block(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self, double* out,
                       cudaStream_t st) {
@@ -662,6 +662,27 @@ void launch_convert(const Ti* in, To* out, long n, cudaStream_t st) {
 }
 template void launch_convert<float, double>(const float*, double*, long, cudaStream_t);
 template void launch_convert<double, float>(const double*, float*, long, cudaStream_t);
+
+template <typename T>
+static cudaError_t prepare_type() {
+    const int bytes = (int)sizeof(LaSmem<T>);
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* fn) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    };
+    set((const void*)k_prior_level<T>);
+    set((const void*)k_finest_group<T>);
+    set((const void*)k_posterior_level<T>);
+    set((const void*)k_predict<T>);
+    set((const void*)k_reduce<T>);
+    set((const void*)k_sample<T>);
+    return e;
+}
+
+cudaError_t prepare_kernels() {
+    cudaError_t e = prepare_type<double>();
+    return e == cudaSuccess ? prepare_type<float>() : e;
+}
 
 #define MRA_INSTANTIATE(T)                                                                                   \
     template void launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t);            \

@@ -94,6 +94,10 @@ struct FieldParams {
 // Sets the text returned by mra_last_error() on this thread.
 void set_last_error(const char* msg);
 
+// Opts the region kernels into their dynamic shared memory size on the current
+// device; call before the first launch (and before any stream capture).
+cudaError_t prepare_kernels();
+
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
 template <typename T>

@@ -1,5 +1,5 @@
-"""The C-ABI library loads and exports every entry point include/mra_b200.h
-declares (no GPU needed: nothing is called)."""
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(no GPU needed: nothing is called)."""
 import ctypes
 import os
 import re
@@ -10,7 +10,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared():
-    text = open(os.path.join(ROOT, "include", "mra_b200.h")).read()
+    inc = os.path.join(ROOT, "include")
+    text = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     return sorted(set(re.findall(r"^\s*(?:mra_status|const char\*)\s+(mra_\w+)\s*\(", text, re.M)))
 
 
