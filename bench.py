@@ -35,7 +35,23 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MRA loglik evals/sec at n=1M (mixed vs plain FP64, same GPU, ≤1e-6 rel err); fit wall-time"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+# per-launch DRAM traffic of the dominant kernels, from ncu captures (see the file)
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.md")
+
+
+def traffic_lookup(key: str):
+    """Bytes per launch for `config:precision:kernel:level` from the table rows
+    "| key | bytes | ... |" of profiles/dram_traffic.md, else None."""
+    if not os.path.exists(TRAFFIC_FILE):
+        return None
+    for line in open(TRAFFIC_FILE):
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 2 and cells[0] == key:
+            try:
+                return float(cells[1])
+            except ValueError:
+                return None
+    return None
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "mra_ref_ext")
 
 
@@ -49,6 +65,8 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-compare", action="store_true",
+                   help="skip timing the other precision on the same inputs")
     return p.parse_args()
 
 
@@ -329,11 +347,32 @@ def main():
     dom = max(launches, key=lambda l: l["ms"])
     achieved = dom["flop"] / (dom["ms"] * 1e-3) / 1e12
     peak = fp64_peak_tflops() if rank == 0 else None
-    traffic = None
-    if os.path.exists(TRAFFIC_FILE):
-        tj = json.load(open(TRAFFIC_FILE))
-        traffic = tj.get(f"{args.config}:{args.precision}:{dom['kernel']}:{dom['level']}")
+    traffic = traffic_lookup(f"{args.config}:{args.precision}:{dom['kernel']}:{dom['level']}")
     ctx.close()
+
+    # the other precision on the same inputs, same GPU (after the first context is freed)
+    other = None
+    if not args.no_compare and world == 1:
+        oprec = "mixed" if args.precision == "fp64" else "fp64"
+        octx = api.Context(st, md, precision=oprec)
+        octx.set_obs_values(y)
+        octx.set_theta()
+        for _ in range(max(args.warmup, 0)):
+            octx.loglik()
+        if not args.no_graph:
+            octx.capture_graph()
+            octx.loglik()
+        torch.cuda.synchronize()
+        octx.timer_start()
+        for _ in range(args.steps):
+            od, oll = octx.loglik()
+        oms = octx.timer_stop()
+        octx.close()
+        fp64_ll = ll if args.precision == "fp64" else oll
+        mixed_ll = oll if args.precision == "fp64" else ll
+        other = {"precision": oprec, "evals_per_s": args.steps / (oms * 1e-3), "ms_per_step": oms / args.steps,
+                 "loglik": oll, "mixed_rel_err_vs_fp64": abs(mixed_ll - fp64_ll) / abs(fp64_ll),
+                 "mixed_speedup_vs_fp64": (ms / oms) if args.precision == "fp64" else (oms / ms)}
 
     if rank != 0:
         if world > 1:
@@ -365,7 +404,8 @@ def main():
                    "cuda_graph": not args.no_graph, "loglik": ll, "d": d, "n_obs": st.n_obs,
                    "setup_seconds": setup_s, "device_gb": stats["bytes_device"] / 1e9,
                    "flop_per_eval": stats["flop_last"],
-                   "stage_ms": {k: stats[k] for k in ("ms_fields", "ms_prior", "ms_finest", "ms_posterior")}},
+                   "stage_ms": {k: stats[k] for k in ("ms_fields", "ms_prior", "ms_finest", "ms_posterior")},
+                   "other_precision": other},
         "roofline": {"bound": "tensor", "kernel": f"{dom['kernel']}(level {dom['level']})",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,

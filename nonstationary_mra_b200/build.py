@@ -42,6 +42,33 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+HOST_SOURCES = ["host/mra_host.cpp"]
+HOST_MAIN = "host/mra_main.cpp"
+HOST_LIB = os.path.join(HERE, "libmra_host.so")
+HOST_EXE = os.path.join(HERE, "mra_b200")
+
+
+def build_host(force: bool = False) -> str:
+    """The C++ host (include/mra_host.hpp): libmra_host.so and the drop-in
+    executable ``mra_b200``, both linked against libmra_b200.so (rpath $ORIGIN)."""
+    build()
+    srcs = [os.path.join(HERE, s) for s in HOST_SOURCES]
+    deps = srcs + [os.path.join(HERE, HOST_MAIN), LIB] + \
+        [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
+    if not force and os.path.exists(HOST_EXE) and os.path.exists(HOST_LIB) and \
+            all(os.path.getmtime(d) <= min(os.path.getmtime(HOST_EXE), os.path.getmtime(HOST_LIB)) for d in deps):
+        return HOST_EXE
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    common = ["-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-L", HERE, "-lmra_b200",
+              "-Wl,-rpath,$ORIGIN"]
+    for cmd in ([cxx, "-shared", "-fPIC", "-o", HOST_LIB] + srcs + common,
+                [cxx, "-o", HOST_EXE, os.path.join(HERE, HOST_MAIN)] + srcs + common):
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"host build failed:\n{res.stderr}")
+    return HOST_EXE
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
     if not force and not needs_build():
         return LIB
@@ -72,3 +99,4 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(verbose="--verbose" in sys.argv, force=True))
+    print(build_host(force=True))

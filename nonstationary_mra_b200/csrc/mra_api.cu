@@ -272,6 +272,7 @@ mra_status run_eval(mra_ctx* c, bool predict) {
                 break;
             case MRA_KERNEL_CONVERT:
                 launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
+                launch_convert<float, double>(tf.Pinv, td.Pinv, c->n_int * rr, st);
                 launch_convert<float, double>(tf.Bhat, td.Bhat, c->n_obs * (long)c->L * c->r, st);
                 break;
             case MRA_KERNEL_POSTERIOR_LEVEL:
@@ -382,8 +383,11 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
             f_sz[m & 1] = std::max(f_sz[m & 1], (size_t)c->n_obs);
         }
     }
-    t.ws_stride = post_part ? std::max((long)r * c->tf + (long)c->tf * c->tf, n_slices(M - 1) * rr + (long)(M - 2) * rr) + 64
+    t.ws_stride = post_part ? std::max((long)r * c->tf + 2L * c->tf * c->tf, n_slices(M - 1) * rr + (long)(M - 2) * rr + rr) + 64
                             : 64;
+    // prior: V of one conditioning step; finest: the inverse of a child's
+    // L_Sigma (n x n, n <= 64, the shared-memory Cholesky's limit)
+    if (prior_part) t.ws_stride = std::max(t.ws_stride, std::max(rr, 64L * 64) + 64);
     t.wsd_stride = post_part ? (long)(M - 1) * r + c->tf + 64 : 64;
     if (!post_part) {
         for (int p = 0; p < 2; ++p) aout_sz[p] = wout_sz[p] = F_sz[p] = f_sz[p] = 1;
@@ -395,6 +399,7 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
         if (ce) return fail(MRA_ERR_OOM, std::string("device allocation failed: ") + #ptr);           \
     } while (0)
     TALLOC(t.Lprior, T, c->n_int * rr);
+    TALLOC(t.Pinv, T, (prior_part || post_part) ? c->n_int * rr : 1);
     TALLOC(t.Bhat, T, c->n_obs * (long)L * r);
     TALLOC(t.U, T, prior_part ? u_total : 1);
     TALLOC(t.Ufin, T, prior_part ? c->n_obs * (long)L * r : 1);

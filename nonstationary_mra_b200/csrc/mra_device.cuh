@@ -71,15 +71,27 @@ __device__ __forceinline__ float matern_f(int nu_x2, float h) {
 
 // C(s1, s2) with per-point sigma^2 (s) and beta (b): evaluate_covariance.cpp:218-225
 // (nonstationary) and :82 (stationary: s1 = sill, b1 = range).
+// For the straight-line distances the scaled distance over sqrt(bbar^2) is
+// taken as sqrt(d^2 / bbar^2) with one reciprocal of bbar^2 shared with the
+// prefactor (one division and one square root fewer than the literal form;
+// the results agree to a few units in the last place).
 __device__ __forceinline__ double cov_entry(const Geom& g, const Pt& p1, double s1, double b1, const Pt& p2,
                                             double s2, double b2) {
-    double D = g.dist_scale * point_distance(g, p1, p2);
-    if (!g.nonstat) return s1 * matern(g.nu_x2, D / b1);
-    double bms = (b1 * b1 + b2 * b2) / 2;
-    double x = (b1 * b2) / bms;
+    if (g.distance == 1 || !g.nonstat) {
+        double D = g.dist_scale * point_distance(g, p1, p2);
+        if (!g.nonstat) return s1 * matern(g.nu_x2, D / b1);
+        double bms = (b1 * b1 + b2 * b2) / 2;
+        double x = (b1 * b2) / bms;
+        double pre = g.pref_kind == 0 ? x * sqrt(x) : (g.pref_kind == 1 ? x : pow(x, g.pref_exp));
+        return sqrt(s1 * s2) * pre * matern(g.nu_x2, D / sqrt(bms));
+    }
+    double dx = p2.c0 - p1.c0, dy = p2.c1 - p1.c1, dz = p2.c2 - p1.c2;
+    double d2 = dx * dx + dy * dy + dz * dz;
+    double ibms = 2.0 / (b1 * b1 + b2 * b2);
+    double x = (b1 * b2) * ibms;
     double pre = g.pref_kind == 0 ? x * sqrt(x) : (g.pref_kind == 1 ? x : pow(x, g.pref_exp));
-    double c = sqrt(s1 * s2) * pre;
-    return c * matern(g.nu_x2, D / sqrt(bms));
+    double h = g.dist_scale * sqrt(d2 * ibms);
+    return sqrt(s1 * s2) * pre * matern(g.nu_x2, h);
 }
 
 // The same entry evaluated in FP32 (the mixed path's covariance evaluation).
@@ -113,22 +125,33 @@ struct PointSet {
 
 // out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
 // diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
+// Thread layout: a fixed row t per thread (its point and fields loaded once),
+// columns strided by the number of row groups; consecutive threads write
+// consecutive rows.
 template <typename T>
-__device__ inline void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self, T* out,
-                                long ld) {
-    for (int e = threadIdx.x; e < na * nb; e += blockDim.x) {
-        int t = e % na, q = e / na;
-        long ia = a0 + t, ib = b0 + q;
-        T v;
-        if (self && t == q) {
-            v = (T)(P.s2[ia] + P.t2[ia]);
-        } else if (sizeof(T) == 8) {
-            v = (T)cov_entry(g, P.pt(ia), P.s2[ia], P.beta[ia], P.pt(ib), P.s2[ib], P.beta[ib]);
-        } else {
-            v = (T)cov_entry_f(g, P.pt(ia), (float)P.s2[ia], (float)P.beta[ia], P.pt(ib), (float)P.s2[ib],
-                               (float)P.beta[ib]);
+__device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
+                                      T* out, long ld) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int rows = na < nt ? na : nt;
+    const int cols = nt / rows;
+    if (tid >= rows * cols) return;
+    const int tr = tid % rows, tq = tid / rows;
+    for (int t = tr; t < na; t += rows) {
+        const long ia = a0 + t;
+        const Pt pa = P.pt(ia);
+        const double sa = P.s2[ia], ba = P.beta[ia];
+        for (int q = tq; q < nb; q += cols) {
+            const long ib = b0 + q;
+            T v;
+            if (self && t == q) {
+                v = (T)(sa + P.t2[ia]);
+            } else if (sizeof(T) == 8) {
+                v = (T)cov_entry(g, pa, sa, ba, P.pt(ib), P.s2[ib], P.beta[ib]);
+            } else {
+                v = (T)cov_entry_f(g, pa, (float)sa, (float)ba, P.pt(ib), (float)P.s2[ib], (float)P.beta[ib]);
+            }
+            out[t + (long)q * ld] = v;
         }
-        out[t + (long)q * ld] = v;
     }
 }
 
@@ -559,6 +582,19 @@ __device__ inline void trsv_lower_f64(int n, const T* L, long ldl, double* b) {
     __syncthreads();
 }
 
+// Deterministic CTA sum (fixed thread -> element mapping and tree order).
+template <typename T>
+__device__ inline double cta_sum(double v, LaSmem<T>& sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) s += sm.red[w];
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+
 // In-place lower Cholesky A = L L^T (strict upper part zeroed, like
 // Armadillo's chol(X, "lower")).  Diagonal blocks and panels in FP64, trailing
 // updates through gemm<T>.  Returns 0, or the 1-based index of the first
@@ -566,7 +602,7 @@ __device__ inline void trsv_lower_f64(int n, const T* L, long ldl, double* b) {
 // with NaNs and the caller reports the region.  *logdet (thread 0) receives
 // 2 * sum(log(diag L)) accumulated in FP64.
 template <typename T>
-__device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* logdet) {
+__device__ inline int potrf_blocked(int n, T* A, long lda, LaSmem<T>& sm, double* logdet) {
     const int tid = threadIdx.x;
     double ld = 0.0;
     if (tid == 0) sm.flag = 0;
@@ -643,17 +679,97 @@ __device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* 
     return sm.flag;
 }
 
-// Deterministic CTA sum (fixed thread -> element mapping and tree order).
+
+// FP64 Cholesky of an n x n matrix, n <= 64, staged whole in shared memory
+// (column-major, ld 65): unblocked right-looking, two barriers per column,
+// column scaling by the reciprocal of the pivot (LAPACK's dpotf2 order).  The
+// log-determinant is summed over the diagonal in parallel at the end.  With
+// `inv` the inverse of the factor is also formed (column j by thread j,
+// forward substitution against the staged factor) and written to inv.
+constexpr int SLD = 65;
+
+__device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm, double* logdet, double* inv,
+                                  long ldinv) {
+    const int tid = threadIdx.x;
+    double* S = &sm.A[0][0];  // 64 x 65 (fits in the operand tile buffers)
+    double* X = &sm.B[0][0];
+    for (int e = tid; e < n * n; e += kThreads) {
+        const int i = e % n, j = e / n;
+        S[i + j * SLD] = A[i + (long)j * lda];
+    }
+    if (tid == 0) sm.flag = 0;
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;
+    for (int k = 0; k < n; ++k) {
+        const double d = S[k + k * SLD];
+        // column k below the pivot, scaled by 1/sqrt(pivot)
+        if (tid > k && tid < n) S[tid + k * SLD] *= 1.0 / sqrt(d);
+        __syncthreads();
+        if (tid == 0) {
+            if (!(d > 0.0) && sm.flag == 0) sm.flag = k + 1;
+            S[k + k * SLD] = sqrt(d);
+        }
+        for (int j = k + 1 + ty; j < n; j += 16) {
+            const double ljk = S[j + k * SLD];
+            for (int i = j + tx; i < n; i += 16) S[i + j * SLD] -= S[i + k * SLD] * ljk;
+        }
+        __syncthreads();
+    }
+    double part = 0.0;
+    for (int i = tid; i < n; i += kThreads) part += log(S[i + i * SLD]);
+    const double sum = cta_sum(part, sm);
+    if (tid == 0 && logdet) *logdet = 2.0 * sum;
+    for (int e = tid; e < n * n; e += kThreads) {
+        const int i = e % n, j = e / n;
+        A[i + (long)j * lda] = i >= j ? S[i + j * SLD] : 0.0;
+    }
+    if (inv) {
+        // X = L^{-1}: thread j solves L x = e_j from row j down
+        if (tid < n) {
+            const int j = tid;
+            for (int i = 0; i < j; ++i) X[i + j * SLD] = 0.0;
+            X[j + j * SLD] = 1.0 / S[j + j * SLD];
+            for (int i = j + 1; i < n; ++i) {
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                int k = j;
+                for (; k + 3 < i; k += 4) {
+                    s0 += S[i + k * SLD] * X[k + j * SLD];
+                    s1 += S[i + (k + 1) * SLD] * X[k + 1 + j * SLD];
+                    s2 += S[i + (k + 2) * SLD] * X[k + 2 + j * SLD];
+                    s3 += S[i + (k + 3) * SLD] * X[k + 3 + j * SLD];
+                }
+                for (; k < i; ++k) s0 += S[i + k * SLD] * X[k + j * SLD];
+                X[i + j * SLD] = -((s0 + s1) + (s2 + s3)) / S[i + i * SLD];
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < n * n; e += kThreads) {
+            const int i = e % n, j = e / n;
+            inv[i + (long)j * ldinv] = X[i + j * SLD];
+        }
+    }
+    __syncthreads();
+    return sm.flag;
+}
+
+// In-place lower Cholesky (see potrf_blocked); FP64 matrices up to 64 go
+// through potrf_small.  With `inv`, L^{-1} is also written there (ld ldinv).
 template <typename T>
-__device__ inline double cta_sum(double v, LaSmem<T>& sm) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < kThreads / 32; ++w) s += sm.red[w];
-    __syncthreads();
-    return s;  // valid in thread 0
+__device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* logdet, T* inv = nullptr,
+                                  long ldinv = 0) {
+    if constexpr (sizeof(T) == 8) {
+        if (n <= 64) return potrf_small(n, A, lda, sm, logdet, inv, ldinv);
+    }
+    const int info = potrf_blocked(n, A, lda, sm, logdet);
+    if (inv) {
+        for (long e = threadIdx.x; e < (long)n * n; e += kThreads) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            inv[i + (long)j * ldinv] = i == j ? (T)1 : (T)0;
+        }
+        __syncthreads();
+        trsm_left_lower<T>(n, n, A, lda, inv, ldinv, sm);
+    }
+    return info;
 }
 
 }  // namespace mra

@@ -88,6 +88,9 @@ __global__ void k_fields(Geom g, FieldParams fp, const double* __restrict__ c0, 
 // ---------------------------------------------------------------------------
 // a5/a6: prior, one level of interior regions
 // ---------------------------------------------------------------------------
+// One CTA per region.  The inverse L_a^{-1} of every prior factor is formed
+// once, right after its Cholesky, so that the m triangular solves of each
+// descendant become tensor-pipe products.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> t, int m) {
     LaSmem<T>& sm = la_smem<T>();
@@ -106,23 +109,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             }
         }
         T* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
+        T* V = t.ws + blockIdx.x * t.ws_stride;   // r x r
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            T* V = Ui + (long)j * r;
-            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, mr);
+            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r);
             __syncthreads();
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, mr, sm);
+                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm);
             }
-            trsm_left_lower<T>(r, r, t.Lprior + a * rr, r, V, mr, sm);
+            // U_{i,j} = L_a^{-1} V as a product with the stored inverse
+            gemm<T, false, false>(r, r, r, (T)1, t.Pinv + a * rr, r, V, r, (T)0, Ui + (long)j * r, mr, sm);
         }
         T* Li = t.Lprior + i * rr;
         fill_cov<T>(g, t.pts, i * r, r, i * r, r, true, Li, r);
         __syncthreads();
         if (m > 0) gemm<T, true, false>(r, r, (int)mr, (T)-1, Ui, mr, Ui, mr, (T)1, Li, r, sm);
         double ld = 0.0;
-        int info = potrf_lower<T>(r, Li, r, sm, &ld);
+        int info = potrf_lower<T>(r, Li, r, sm, &ld, t.Pinv + i * rr, r);
         if (threadIdx.x == 0) {
             t.ldprior[i] = ld;
             if (info) report_error(t.err, i);
@@ -136,24 +140,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
 // Factored input (F: n rows of width (m+1) r, row stride ldF; f: n doubles).
 // Writes F' (n rows of width m r) to Fo and f' to fo when m > 0.
 template <typename T>
-__device__ void factored_step(const DevTree<T>& t, int m, long i, int n, const T* F, long ldF, const double* f, T* Fo,
+__device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, int n, const T* F, long ldF, const double* f, T* Fo,
                               double* fo, bool keep, T* ws, double* wsd, LaSmem<T>& sm, double& dterm) {
     const int r = t.r;
     const long rr = (long)r * r, mr = (long)m * r;
     const T* Li = t.Lprior + i * rr;
     T* Y = ws;                  // r x n
     T* S = ws + (long)r * n;    // n x n
-    for (long e = threadIdx.x; e < (long)r * n; e += kThreads) {
-        int tt = (int)(e % r), q = (int)(e / r);
-        Y[e] = F[(long)q * ldF + mr + tt];
-    }
-    __syncthreads();
-    trsm_left_lower<T>(r, n, Li, r, Y, r, sm);
+    T* Rinv = S + (long)n * n;  // n x n (n <= 64)
+    // Y = L_i^{-1} F_m^T as a product with the stored inverse of the prior factor
+    gemm<T, false, false>(r, n, r, (T)1, t.Pinv + i * rr, r, F + mr, ldF, (T)0, Y, r, sm);
     gemm<T, true, false>(n, n, r, (T)1, Y, r, Y, r, (T)0, S, n, sm);
     for (int q = threadIdx.x; q < n; q += kThreads) S[q + (long)q * n] += (T)1;
     __syncthreads();
     double ld = 0.0;
-    int info = potrf_lower<T>(n, S, n, sm, &ld);
+    const bool small = sizeof(T) == 8 && n <= 64;
+    int info = potrf_lower<T>(n, S, n, sm, &ld, small ? Rinv : nullptr, n);
     double* fp = m > 0 ? fo : wsd;
     double part = 0.0;
     for (int q = threadIdx.x; q < n; q += kThreads) {
@@ -170,12 +172,17 @@ __device__ void factored_step(const DevTree<T>& t, int m, long i, int n, const T
         if (info) report_error(t.err, i);
     }
     if (m > 0) {
-        for (long e = threadIdx.x; e < mr * n; e += kThreads) {
-            long x = e % mr, q = e / mr;
-            Fo[q * mr + x] = F[q * ldF + x];
+        if (small) {
+            // F' = F_{0..m-1} R^{-T}
+            gemm<T, false, true>((int)mr, n, n, (T)1, F, ldF, Rinv, n, (T)0, Fo, mr, sm);
+        } else {
+            for (long e = threadIdx.x; e < mr * n; e += kThreads) {
+                long x = e % mr, q = e / mr;
+                Fo[q * mr + x] = F[q * ldF + x];
+            }
+            __syncthreads();
+            trsm_right_lower_trans<T>((int)mr, n, S, n, Fo, mr, sm);
         }
-        __syncthreads();
-        trsm_right_lower_trans<T>((int)mr, n, S, n, Fo, mr, sm);
     }
     if (keep) {
         // predictive factors of the region: L~ L~^T = L L^T + F_m^T F_m, v = L~^{-1} F_m^T f,
@@ -204,7 +211,7 @@ __device__ void factored_step(const DevTree<T>& t, int m, long i, int n, const T
 // Dense input: Aagg holds the slices (j,k), j <= k <= m, of the summed children
 // contributions, wagg the (m+1) x r summed w.
 template <typename T>
-__device__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, const double* wagg, bool keep, T* Gw,
+__device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, const double* wagg, bool keep, T* Gw,
                            LaSmem<T>& sm, double& dterm) {
     const int r = t.r;
     const long rr = (long)r * r, mr = (long)m * r;
@@ -216,7 +223,9 @@ __device__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, co
     for (long e = threadIdx.x; e < rr; e += kThreads) Lt[e] += Amm[e];
     __syncthreads();
     double ld = 0.0;
-    int info = potrf_lower<T>(r, Lt, r, sm, &ld);
+    T* Ltinv = Gw + mr * r;  // r x r scratch after the G scratch
+    const bool small = sizeof(T) == 8 && r <= 64 && m > 0;
+    int info = potrf_lower<T>(r, Lt, r, sm, &ld, small ? Ltinv : nullptr, r);
     double* v = t.vpost + i * r;
     for (int e = threadIdx.x; e < r; e += kThreads) v[e] = wagg[mr + e];
     __syncthreads();
@@ -230,14 +239,21 @@ __device__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, co
     }
     if (m == 0) return;
     T* Gi = keep ? t.G + t.u_off[m] + loc * mr * r : Gw;  // r x (m r), ld = r
-    for (long e = threadIdx.x; e < mr * r; e += kThreads) {
-        int j = (int)(e / rr);
-        long w = e % rr;
-        int p = (int)(w % r), q = (int)(w / r);
-        Gi[e] = Aagg[slice_index(m + 1, j, m) * rr + q + (long)p * r];  // G_j = A_(j,m)^T
+    if (small) {
+        // G_j = L~^{-1} A_(j,m)^T
+        for (int j = 0; j < m; ++j)
+            gemm<T, false, true>(r, r, r, (T)1, Ltinv, r, Aagg + slice_index(m + 1, j, m) * rr, r, (T)0,
+                                 Gi + (long)j * rr, r, sm);
+    } else {
+        for (long e = threadIdx.x; e < mr * r; e += kThreads) {
+            int j = (int)(e / rr);
+            long w = e % rr;
+            int p = (int)(w % r), q = (int)(w / r);
+            Gi[e] = Aagg[slice_index(m + 1, j, m) * rr + q + (long)p * r];  // G_j = A_(j,m)^T
+        }
+        __syncthreads();
+        trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
     }
-    __syncthreads();
-    trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
     double* wo = t.wout[m & 1] + loc * mr;
     for (long x = threadIdx.x; x < mr; x += kThreads) {
         double s = 0.0;
@@ -258,7 +274,7 @@ __device__ void dense_step(const DevTree<T>& t, int m, long i, const T* Aagg, co
 
 // Aagg/wagg += the (A~, w~) of factored rows F (n x (m+1) r, row stride ldF), f.
 template <typename T>
-__device__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* F, long ldF, const double* f, T* Aagg,
+__device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* F, long ldF, const double* f, T* Aagg,
                                     double* wagg, LaSmem<T>& sm) {
     const int r = t.r;
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
@@ -315,20 +331,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
             T* Bh = t.Bhat + lo * Lr;
             for (int j = 0; j < L; ++j) {
                 const long a = anc[j];
-                T* V = Uf + (long)j * r;
+                T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
                 fill_cov<T>(g, t.pts, a * r, r, t.obs0 + lo, np, false, V, Lr);
                 __syncthreads();
                 if (j > 0) {
                     const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                     gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, Uf, Lr, (T)1, V, Lr, sm);
                 }
-                for (long e = threadIdx.x; e < (long)r * np; e += kThreads) {
-                    int tt = (int)(e % r);
-                    long q = e / r;
-                    Bh[(long)j * r + tt + q * Lr] = V[tt + q * Lr];
-                }
-                __syncthreads();
-                trsm_left_lower<T>(r, np, t.Lprior + a * rr, r, V, Lr, sm);
+                gemm<T, false, false>(r, np, r, (T)1, t.Pinv + a * rr, r, V, Lr, (T)0, Uf + (long)j * r, Lr, sm);
             }
             for (long c = clo; c < chi; ++c) {
                 const long o0 = t.obs_off[c];
@@ -340,12 +350,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
                 gemm<T, true, false>(n, n, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, t.Ufin + o0 * Lr, Lr, (T)1, S, n,
                                      sm);
                 double ld = 0.0;
-                int info = potrf_lower<T>(n, S, n, sm, &ld);
+                const bool small = sizeof(T) == 8 && n <= 64;
+                T* Sinv = ws;  // n x n
+                int info = potrf_lower<T>(n, S, n, sm, &ld, small ? Sinv : nullptr, n);
                 double* ytc = t.yt + o0;
                 for (int e = threadIdx.x; e < n; e += kThreads) ytc[e] = t.y[o0 + e];
                 __syncthreads();
                 trsv_lower_f64<T>(n, S, n, ytc);
-                trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
+                if (small) {
+                    // B^ = V L_Sigma^{-T}, in place: each 64-row tile of the product
+                    // reads exactly the rows it then writes
+                    gemm<T, false, true>((int)Lr, n, n, (T)1, t.Bhat + o0 * Lr, Lr, Sinv, n, (T)0, t.Bhat + o0 * Lr,
+                                         Lr, sm);
+                } else {
+                    trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
+                }
                 double part = 0.0;
                 for (int e = threadIdx.x; e < n; e += kThreads) part += ytc[e] * ytc[e];
                 double yy = cta_sum(part, sm);

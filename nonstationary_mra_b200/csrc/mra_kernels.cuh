@@ -34,6 +34,7 @@ struct DevTree {
     int64_t u_off[kMaxLevels]; // offset of level m's U (= G) blocks, m*r*r per region
     // prior
     T* Lprior;                 // [n_int][r*r]
+    T* Pinv;                   // [n_int][r*r] inverse of each prior factor (L^{-1} applied as a product)
     double* ldprior;           // [n_int] 2 sum log diag of the prior factor
     T* U;                      // per level m: [J^m][(m r) x r], ld = m r
     T* Ufin;                   // [n_obs][L r]   finest U_{k,j} columns, obs-major

@@ -154,72 +154,72 @@ __global__ void __launch_bounds__(H) k_mlp_pass(MlpArgs a) {
                 if (h == 0 && s < ns) a.Y[s0 + s] = y;
             }
         }
-        if (MODE == PREDICT) {
+        if constexpr (MODE == PREDICT) {
             __syncthreads();
-            continue;
-        }
-        // backward through the output layer
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            float sg = sigm(z2[s]);
-            float a2 = z2[s] * sg;
-            float g = gy[s] * w3h * (sg * (1.f + z2[s] * (1.f - sg)));
-            gzs[s * H + h] = g;
-            if (MODE == TRAIN) {
-                dw3 = fmaf(gy[s], a2, dw3);
-                db2 += g;
-                if (h == 0) db3 += gy[s];
-            }
-        }
-        __syncthreads();
-        float a1h[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) a1h[s] = a1s[s * H + h];
-        if (MODE == TRAIN) {
-            for (int o = 0; o < H; ++o) {
-                float acc = 0.f;
-#pragma unroll
-                for (int s = 0; s < S; ++s) acc = fmaf(gzs[s * H + o], a1h[s], acc);
-                dW2[o * H + h] += acc;
-            }
-        }
-        // through W2 and the first activation
-        float gz1[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) gz1[s] = 0.f;
-        for (int o = 0; o < H; ++o) {
-            float w = __bfloat162float(W2s[o * H + h]);
-#pragma unroll
-            for (int s = 0; s < S; ++s) gz1[s] = fmaf(w, gzs[s * H + o], gz1[s]);
-        }
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            float sg = sigm(z1[s]);
-            gz1[s] *= sg * (1.f + z1[s] * (1.f - sg));
-        }
-        if (MODE == TRAIN) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) db1 += gz1[s];
-            for (int d = 0; d < D; ++d) {
-                float acc = 0.f;
-#pragma unroll
-                for (int s = 0; s < S; ++s) acc = fmaf(gz1[s], xs[s * MAXD + d], acc);
-                dW1[d * H + h] += acc;
-            }
         } else {
-            // d y / d x: sum over hidden units of W1[h][d] g_z1[h]
-            __syncthreads();
+            // backward through the output layer
 #pragma unroll
-            for (int s = 0; s < S; ++s) gzs[s * H + h] = gz1[s];
-            __syncthreads();
-            for (int e = h; e < S * D; e += H) {
-                int s = e / D, d = e % D;
-                float acc = 0.f;
-                for (int k = 0; k < H; ++k) acc = fmaf(__bfloat162float(W1t[d * H + k]), gzs[s * H + k], acc);
-                if (s < ns) a.G[(s0 + s) * D + d] = acc;
+            for (int s = 0; s < S; ++s) {
+                float sg = sigm(z2[s]);
+                float a2 = z2[s] * sg;
+                float g = gy[s] * w3h * (sg * (1.f + z2[s] * (1.f - sg)));
+                gzs[s * H + h] = g;
+                if (MODE == TRAIN) {
+                    dw3 = fmaf(gy[s], a2, dw3);
+                    db2 += g;
+                    if (h == 0) db3 += gy[s];
+                }
             }
+            __syncthreads();
+            float a1h[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) a1h[s] = a1s[s * H + h];
+            if (MODE == TRAIN) {
+                for (int o = 0; o < H; ++o) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int s = 0; s < S; ++s) acc = fmaf(gzs[s * H + o], a1h[s], acc);
+                    dW2[o * H + h] += acc;
+                }
+            }
+            // through W2 and the first activation
+            float gz1[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) gz1[s] = 0.f;
+            for (int o = 0; o < H; ++o) {
+                float w = __bfloat162float(W2s[o * H + h]);
+#pragma unroll
+                for (int s = 0; s < S; ++s) gz1[s] = fmaf(w, gzs[s * H + o], gz1[s]);
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                float sg = sigm(z1[s]);
+                gz1[s] *= sg * (1.f + z1[s] * (1.f - sg));
+            }
+            if (MODE == TRAIN) {
+#pragma unroll
+                for (int s = 0; s < S; ++s) db1 += gz1[s];
+                for (int d = 0; d < D; ++d) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int s = 0; s < S; ++s) acc = fmaf(gz1[s], xs[s * MAXD + d], acc);
+                    dW1[d * H + h] += acc;
+                }
+            } else {
+                // d y / d x: sum over hidden units of W1[h][d] g_z1[h]
+                __syncthreads();
+#pragma unroll
+                for (int s = 0; s < S; ++s) gzs[s * H + h] = gz1[s];
+                __syncthreads();
+                for (int e = h; e < S * D; e += H) {
+                    int s = e / D, d = e % D;
+                    float acc = 0.f;
+                    for (int k = 0; k < H; ++k) acc = fmaf(__bfloat162float(W1t[d * H + k]), gzs[s * H + k], acc);
+                    if (s < ns) a.G[(s0 + s) * D + d] = acc;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
     if (MODE != TRAIN) return;
     float* out = a.partial + (long)blockIdx.x * (a.P + 1);

@@ -87,3 +87,43 @@ def test_training_fits_a_smooth_target():
     np.testing.assert_array_equal(net.params(), net2.params())
     net.close()
     net2.close()
+
+
+def test_trained_network_ranks_unseen_parameters():
+    """What the network adds over the exact method alone: trained on exact
+    (theta, loglik) pairs, it orders parameter vectors it has not seen by their
+    exact log-likelihood without evaluating them (Spearman correlation), so the
+    fitting loop can spend exact evaluations on its best candidates only."""
+    from nonstationary_mra_b200 import api, partition, synth
+    from nonstationary_mra_b200.fit import NonstationaryObjective
+    rng = np.random.default_rng(21)
+    cfg = synth.Config("s", 2048, 4, 4, 16, 1, 8, "uniform", 0.3, 21)
+    xy, _ = synth.locations(cfg, rng)
+    theta = synth.true_theta(cfg, rng)
+    md = synth.model_from_theta(theta, 1)
+    st = partition.build_by_program(xy[0], xy[1], np.zeros(cfg.n), 4, 4, 16, np.e / 100, distance=2)
+    ctx = api.Context(st, md)
+    ctx.set_theta()
+    st.obs_value = ctx.sample_prior(rng.standard_normal(st.n_interior * st.r), rng.standard_normal(st.n_obs))
+    ctx.set_obs_values(st.obs_value)
+    obj = NonstationaryObjective(ctx, 0.0, float(np.log(0.1)))
+    t0 = synth.theta_vector(theta)
+    pts = t0 + rng.uniform(-0.4, 0.4, size=(264, N_IN))
+    ll = np.array([obj.loglik(p) for p in pts])
+    tr, te = slice(0, 200), slice(200, 264)
+    scale = 0.4
+    x = ((pts - t0) / scale).astype(np.float32)
+    mu, sd = ll[tr].mean(), ll[tr].std()
+    net = Surrogate(N_IN, seed=7)
+    net.set_data(x[tr], ((ll[tr] - mu) / sd).astype(np.float32))
+    net.train(3000, 2e-3)
+    pred = net.predict(x[te])
+    rank = lambda a: np.argsort(np.argsort(a))
+    rho = np.corrcoef(rank(pred), rank(ll[te]))[0, 1]
+    print(f"Spearman rank correlation on unseen parameters: {rho:.3f}")
+    assert rho > 0.5, rho
+    # the network's top quarter is better, by exact loglik, than the rest
+    top = np.argsort(-pred)[:16]
+    assert ll[te][top].mean() > ll[te].mean()
+    net.close()
+    ctx.close()
