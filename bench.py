@@ -65,6 +65,10 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--fit", action="store_true",
+                   help="instead of the log-likelihood line: fit wall-time of the plain optimizer vs the "
+                        "surrogate-assisted one (19 nonstationary parameters, c2 layout)")
+    p.add_argument("--fit-evals", type=int, default=2000)
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -273,11 +277,58 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+def fit_arm(args):
+    """Surrogate-assisted fitting vs the plain optimizer from the same seeded
+    theta0 on the exact GPU log-likelihood: wall time of each to reach the
+    plain optimizer's final log-likelihood (within 1e-6 relative)."""
+    from nonstationary_mra_b200 import api, synth
+    from nonstationary_mra_b200.fit import FitConfig, NonstationaryObjective, fit_plain, fit_surrogate
+    cfg = synth.CONFIGS["c2" if args.config == "c3" else args.config]
+    xy, pred, theta, md, st = make_problem(cfg)
+    ctx = api.Context(st, md)
+    y = draw_values(ctx, st, cfg.seed + 7)
+    ctx.set_obs_values(y)
+    ctx.set_theta()
+    ctx.capture_graph()
+    rng = np.random.Generator(np.random.PCG64(cfg.seed + 11))
+    th0 = np.concatenate([0.3 * rng.standard_normal(9), cfg.range_sd * rng.standard_normal(9), [np.log(0.1)]])
+    lo = np.concatenate([-2.5 * np.ones(18), [np.log(1e-3)]])
+    hi = np.concatenate([2.5 * np.ones(18), [0.0]])
+    icpt = (0.0, float(np.log(0.1)))
+    fc = FitConfig(max_evals=args.fit_evals)
+    plain = NonstationaryObjective(ctx, *icpt)
+    t = time.perf_counter()
+    fit_plain(plain, th0, lo, hi, fc)
+    t_plain = time.perf_counter() - t
+    L = plain.trace.best_loglik()
+    target = L - 1e-6 * abs(L)
+    sur = NonstationaryObjective(ctx, *icpt)
+    t = time.perf_counter()
+    _, L_sur, info = fit_surrogate(sur, th0, lo, hi, fc)
+    t_sur = time.perf_counter() - t
+    ctx.close()
+    reach = sur.trace.time_to_reach(target)
+    line = {"metric": "fit wall-time to the plain optimizer's final loglik (within 1e-6 relative)",
+            "value": reach, "unit": "s", "higher_is_better": False,
+            "config": {"workload": workload_name(cfg) + ", theta = 9 log-sigma + 9 log-range + log tau^2",
+                       "max_evals": args.fit_evals, "n_train": fc.n_train},
+            "plain": {"seconds": t_plain, "evals": len(plain.trace.loglik), "loglik": L},
+            "surrogate": {"seconds": t_sur, "evals": info["evals"], "loglik": L_sur,
+                          "proposals": info["proposals"], "accepted": info["accepted"],
+                          "seconds_to_plain_final": reach,
+                          "evals_to_plain_final": sur.trace.evals_to_reach(target)},
+            "ratio_to_plain": (reach / t_plain) if reach else None}
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def main():
     args = parse_args()
+    if args.fit:
+        fit_arm(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
