@@ -700,20 +700,60 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
     if (tid == 0) sm.flag = 0;
     __syncthreads();
     const int tx = tid & 15, ty = tid >> 4;
-    for (int k = 0; k < n; ++k) {
-        const double d = S[k + k * SLD];
-        // column k below the pivot, scaled by 1/sqrt(pivot)
-        if (tid > k && tid < n) S[tid + k * SLD] *= 1.0 / sqrt(d);
-        __syncthreads();
-        if (tid == 0) {
-            if (!(d > 0.0) && sm.flag == 0) sm.flag = k + 1;
-            S[k + k * SLD] = sqrt(d);
+    for (int b0 = 0; b0 < n; b0 += NB) {
+        const int nb = min(NB, n - b0);
+        // diagonal block by warp 0, lane i owning row b0+i (right-looking)
+        if (tid < 32) {
+            const int lane = tid;
+            double* D = S + b0 + b0 * SLD;
+            for (int k = 0; k < nb; ++k) {
+                if (lane == 0) {
+                    const double d = D[k + k * SLD];
+                    if (!(d > 0.0) && sm.flag == 0) sm.flag = b0 + k + 1;
+                    const double sq = sqrt(d);
+                    D[k + k * SLD] = sq;
+                    sm.inv[k] = 1.0 / sq;
+                }
+                __syncwarp();
+                if (lane > k && lane < nb) D[lane + k * SLD] *= sm.inv[k];
+                __syncwarp();
+                if (lane > k && lane < nb) {
+                    const double lik = D[lane + k * SLD];
+                    for (int j = k + 1; j <= lane; ++j) D[lane + j * SLD] -= lik * D[j + k * SLD];
+                }
+                __syncwarp();
+            }
         }
-        for (int j = k + 1 + ty; j < n; j += 16) {
-            const double ljk = S[j + k * SLD];
-            for (int i = j + tx; i < n; i += 16) S[i + j * SLD] -= S[i + k * SLD] * ljk;
-        }
         __syncthreads();
+        if (b0 + nb < n) {
+            // panel: each row below solves x L_d^T = a against the diagonal block
+            for (int i = b0 + nb + tid; i < n; i += kThreads) {
+                double x[NB];
+#pragma unroll
+                for (int k = 0; k < NB; ++k) x[k] = k < nb ? S[i + (b0 + k) * SLD] : 0.0;
+#pragma unroll
+                for (int k = 0; k < NB; ++k) {
+                    if (k < nb) {
+                        double v = x[k];
+#pragma unroll
+                        for (int c = 0; c < k; ++c) v -= x[c] * S[(b0 + k) + (b0 + c) * SLD];
+                        x[k] = v * sm.inv[k];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NB; ++k)
+                    if (k < nb) S[i + (b0 + k) * SLD] = x[k];
+            }
+            __syncthreads();
+            // trailing rank-nb update of the lower triangle
+            for (int j = b0 + nb + ty; j < n; j += 16)
+                for (int i = j + tx; i < n; i += 16) {
+                    double v = 0.0;
+                    for (int c = 0; c < nb; ++c) v += S[i + (b0 + c) * SLD] * S[j + (b0 + c) * SLD];
+                    S[i + j * SLD] -= v;
+                }
+            __syncthreads();
+        }
     }
     double part = 0.0;
     for (int i = tid; i < n; i += kThreads) part += log(S[i + i * SLD]);
