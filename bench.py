@@ -435,7 +435,7 @@ def main():
         try:
             r = run_cpu_reference(cfg, 3, 1, ctx_factory=lambda s, m: api.Context(s, m))
             t = statistics.median(r["secs"])
-            f_full = stats["flop_last"]
+            f_full = canonical_flops(st)  # the reference algorithm's work, as in the reference arm
             sc = r["sample"]
             cpu = {"value": 1.0 / (t * f_full / r["f_sample"]), "unit": "evals/s", "cores": r["cores"],
                    "kind": r["kind"],

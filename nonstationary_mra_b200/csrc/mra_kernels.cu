@@ -292,6 +292,105 @@ __device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int
 }
 
 // ---------------------------------------------------------------------------
+// a7/a8: the finest children of one level M-2 region, all at once
+// ---------------------------------------------------------------------------
+// Used when every child has at most 32 observations and the group at most 64
+// (T = double): one covariance block and one product form the whole group's
+// conditional covariance, one warp per child factors its diagonal block,
+// solves y~ and inverts its factor into a block-diagonal matrix, and one
+// product forms the whole group's B^ (in place: each 64-row tile of the
+// product reads exactly the rows it then writes, and the group fits one
+// column tile).  Returns the group's log-likelihood terms (thread 0).
+constexpr int kGroupMax = 64;
+constexpr int kChildMax = 32;
+
+template <typename T>
+__device__ __noinline__ double finest_children_grouped(const Geom& g, const DevTree<T>& t, long clo, long chi,
+                                                       long lo, int np, T* ws, LaSmem<T>& sm) {
+    if constexpr (sizeof(T) != 8) {
+        return 0.0;
+    } else {
+        const long Lr = (long)t.L * t.r;
+        const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+        T* Sg = ws;                      // np x np conditional covariance of the group
+        T* Binv = ws + (long)np * np;    // np x np block-diagonal L_Sigma^{-1}
+        fill_cov<T>(g, t.pts, t.obs0 + lo, np, t.obs0 + lo, np, true, Sg, np);
+        for (int e = tid; e < np * np; e += kThreads) Binv[e] = 0.0;
+        __syncthreads();
+        gemm<T, true, false>(np, np, (int)Lr, (T)-1, t.Ufin + lo * Lr, Lr, t.Ufin + lo * Lr, Lr, (T)1, Sg, np, sm);
+        constexpr int LD = kChildMax + 1;
+        double* Sw = &sm.A[0][0] + w * (kChildMax * LD);  // per-warp 32 x 33 (A and B tiles are contiguous)
+        double part = 0.0;
+        const long c = clo + w;
+        if (c < chi) {
+            const long o0 = t.obs_off[c];
+            const int n = (int)(t.obs_off[c + 1] - o0), q0 = (int)(o0 - lo);
+            if (n > 0) {
+                for (int e = lane; e < n * n; e += 32) {
+                    const int i = e % n, j = e / n;
+                    Sw[i + j * LD] = Sg[(q0 + i) + (long)(q0 + j) * np];
+                }
+                __syncwarp();
+                int bad = 0;
+                for (int k = 0; k < n; ++k) {  // lane i owns row i
+                    const double d = Sw[k + k * LD];
+                    __syncwarp();
+                    if (!(d > 0.0)) bad = 1;
+                    const double sq = sqrt(d);
+                    if (lane == k) Sw[k + k * LD] = sq;
+                    if (lane > k && lane < n) Sw[lane + k * LD] *= 1.0 / sq;
+                    __syncwarp();
+                    if (lane > k && lane < n) {
+                        const double lik = Sw[lane + k * LD];
+                        for (int j = k + 1; j <= lane; ++j) Sw[lane + j * LD] -= lik * Sw[j + k * LD];
+                    }
+                    __syncwarp();
+                }
+                T* Lc = t.Lsig + t.lsig_off[c];
+                for (int e = lane; e < n * n; e += 32) {
+                    const int i = e % n, j = e / n;
+                    Lc[i + (long)j * n] = i >= j ? Sw[i + j * LD] : 0.0;
+                }
+                double ldp = lane < n ? log(Sw[lane + lane * LD]) : 0.0;
+                for (int o = 16; o > 0; o >>= 1) ldp += __shfl_xor_sync(0xffffffffu, ldp, o);
+                // y~ = L_Sigma^{-1} y: lane i ends holding x_i
+                double xl = 0.0;
+                for (int i = 0; i < n; ++i) {
+                    double sp = lane < i ? Sw[i + lane * LD] * xl : 0.0;
+                    for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+                    if (lane == i) xl = (t.y[o0 + i] - sp) / Sw[i + i * LD];
+                }
+                if (lane < n) t.yt[o0 + lane] = xl;
+                double yy = lane < n ? xl * xl : 0.0;
+                for (int o = 16; o > 0; o >>= 1) yy += __shfl_xor_sync(0xffffffffu, yy, o);
+                // column j of L_Sigma^{-1} by lane j, into the child's diagonal block
+                if (lane < n) {
+                    const int j = lane;
+                    T* X = Binv + q0 + (long)(q0 + j) * np;  // X[i] = row q0+i of column q0+j
+                    X[j] = 1.0 / Sw[j + j * LD];
+                    for (int i = j + 1; i < n; ++i) {
+                        double v = 0.0;
+                        for (int k = j; k < i; ++k) v += Sw[i + k * LD] * X[k];
+                        X[i] = -v / Sw[i + i * LD];
+                    }
+                }
+                part = yy + 2.0 * ldp;
+                if (bad && lane == 0) report_error(t.err, t.n_int + c);
+            }
+        }
+        __syncthreads();
+        if (lane == 0) sm.red[w] = part;
+        __syncthreads();
+        double tot = 0.0;
+        if (tid == 0)
+            for (int k = 0; k < kThreads / 32; ++k) tot += sm.red[k];
+        __syncthreads();
+        gemm<T, false, true>((int)Lr, np, np, (T)1, t.Bhat + lo * Lr, Lr, Binv, np, (T)0, t.Bhat + lo * Lr, Lr, sm);
+        return tot;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // a7/a8 (+ a9 at level M-2): finest level, one CTA per sibling group
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -340,7 +439,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
                 }
                 gemm<T, false, false>(r, np, r, (T)1, t.Pinv + a * rr, r, V, Lr, (T)0, Uf + (long)j * r, Lr, sm);
             }
-            for (long c = clo; c < chi; ++c) {
+            int nmax = 0;
+            for (long c = clo; c < chi; ++c) nmax = max(nmax, (int)(t.obs_off[c + 1] - t.obs_off[c]));
+            const bool grouped = sizeof(T) == 8 && nmax <= kChildMax && np <= kGroupMax &&
+                                 chi - clo <= kThreads / 32;
+            if (grouped) dterm += finest_children_grouped<T>(g, t, clo, chi, lo, np, ws, sm);
+            for (long c = clo; c < chi && !grouped; ++c) {
                 const long o0 = t.obs_off[c];
                 const int n = (int)(t.obs_off[c + 1] - o0);
                 if (n == 0) continue;

@@ -217,7 +217,7 @@ class FitConfig:
     starts: int = 64            # multi-start ascent on the network
     ascent_steps: int = 60
     keep_best: int = 160        # training set size
-    train_set: str = "nearest"  # "nearest": pairs closest to the best point; "best": highest loglik
+    train_set: str = "best"     # "best": highest loglik; "nearest": pairs closest to the best point
     proposal: str = "ball"      # "ball": gradient path in an L2 trust region; "box": multi-start in a box
     seed: int = 0
 
