@@ -123,37 +123,6 @@ struct PointSet {
     __device__ __forceinline__ Pt pt(long i) const { return Pt{c0[i], c1[i], c2[i]}; }
 };
 
-// out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
-// diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
-// Thread layout: a fixed row t per thread (its point and fields loaded once),
-// columns strided by the number of row groups; consecutive threads write
-// consecutive rows.
-template <typename T>
-__device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
-                                      T* out, long ld) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int rows = na < nt ? na : nt;
-    const int cols = nt / rows;
-    if (tid >= rows * cols) return;
-    const int tr = tid % rows, tq = tid / rows;
-    for (int t = tr; t < na; t += rows) {
-        const long ia = a0 + t;
-        const Pt pa = P.pt(ia);
-        const double sa = P.s2[ia], ba = P.beta[ia];
-        for (int q = tq; q < nb; q += cols) {
-            const long ib = b0 + q;
-            T v;
-            if (self && t == q) {
-                v = (T)(sa + P.t2[ia]);
-            } else if (sizeof(T) == 8) {
-                v = (T)cov_entry(g, pa, sa, ba, P.pt(ib), P.s2[ib], P.beta[ib]);
-            } else {
-                v = (T)cov_entry_f(g, pa, (float)sa, (float)ba, P.pt(ib), (float)P.s2[ib], (float)P.beta[ib]);
-            }
-            out[t + (long)q * ld] = v;
-        }
-    }
-}
 
 // ----------------------------------------------------------------------------
 // tensor-pipe fragments
@@ -232,6 +201,75 @@ template <typename T>
 __device__ __forceinline__ LaSmem<T>& la_smem() {
     extern __shared__ __align__(16) unsigned char la_dyn_smem[];
     return *reinterpret_cast<LaSmem<T>*>(la_dyn_smem);
+}
+
+// out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
+// diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
+// The column points (coordinates, sqrt(sigma^2), beta) are staged in shared
+// memory in chunks, each thread keeps one row point in registers and walks
+// columns strided by the number of row groups (consecutive threads write
+// consecutive rows).  For the straight-line nonstationary case the entry is
+// sqrt(s1) sqrt(s2) pre(x) matern(h) with x = 2 b1 b2 / (b1^2 + b2^2) and
+// h = scale sqrt(2 d^2 / (b1^2 + b2^2)): one division, one square root and
+// one exponential per entry.  Ends with a barrier; uses the tile buffers of sm.
+template <typename T>
+__device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
+                                      T* out, long ld, LaSmem<T>& sm) {
+    constexpr int CH = sizeof(T) == 8 ? 512 : 96;  // columns staged per chunk
+    double* sx = reinterpret_cast<double*>(&sm.A[0][0]);
+    double* sy = sx + CH;
+    double* sz = sy + CH;
+    double* ss = sz + CH;
+    double* sb = ss + CH;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int rows = na < nt ? na : nt;
+    const int cols = nt / rows;
+    const bool worker = tid < rows * cols;
+    const int tr = tid % rows, tq = tid / rows;
+    const bool fast = sizeof(T) == 8 && g.nonstat && g.distance != 1;
+    for (int q0 = 0; q0 < nb; q0 += CH) {
+        const int qn = nb - q0 < CH ? nb - q0 : CH;
+        __syncthreads();
+        for (int e = tid; e < qn; e += nt) {
+            const long ib = b0 + q0 + e;
+            sx[e] = P.c0[ib];
+            sy[e] = P.c1[ib];
+            sz[e] = P.c2[ib];
+            ss[e] = fast ? sqrt(P.s2[ib]) : P.s2[ib];
+            sb[e] = P.beta[ib];
+        }
+        __syncthreads();
+        if (!worker) continue;
+        for (int t = tr; t < na; t += rows) {
+            const long ia = a0 + t;
+            const Pt pa = P.pt(ia);
+            const double sa = P.s2[ia], ba = P.beta[ia];
+            const double ssa = sqrt(sa), ba2 = ba * ba;
+#pragma unroll 4
+            for (int q = tq; q < qn; q += cols) {
+                const int qq = q0 + q;
+                T v;
+                if (self && t == qq) {
+                    v = (T)(sa + P.t2[ia]);
+                } else if (fast) {
+                    const double dx = sx[q] - pa.c0, dy = sy[q] - pa.c1, dz = sz[q] - pa.c2;
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    const double bb = sb[q];
+                    const double ibms = 2.0 / (ba2 + bb * bb);
+                    const double x = (ba * bb) * ibms;
+                    const double pre = g.pref_kind == 0 ? x * sqrt(x) : (g.pref_kind == 1 ? x : pow(x, g.pref_exp));
+                    v = (T)(ssa * ss[q] * pre * matern(g.nu_x2, g.dist_scale * sqrt(d2 * ibms)));
+                } else if (sizeof(T) == 8) {
+                    v = (T)cov_entry(g, pa, sa, ba, Pt{sx[q], sy[q], sz[q]}, ss[q], sb[q]);
+                } else {
+                    v = (T)cov_entry_f(g, pa, (float)sa, (float)ba, Pt{sx[q], sy[q], sz[q]}, (float)ss[q],
+                                       (float)sb[q]);
+                }
+                out[t + (long)qq * ld] = v;
+            }
+        }
+    }
+    __syncthreads();
 }
 
 // ---- FP64: warp tile (8 NW) rows x 16 columns --------------------------------
@@ -717,10 +755,10 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
                 __syncwarp();
                 if (lane > k && lane < nb) D[lane + k * SLD] *= sm.inv[k];
                 __syncwarp();
-                if (lane > k && lane < nb) {
-                    const double lik = D[lane + k * SLD];
-                    for (int j = k + 1; j <= lane; ++j) D[lane + j * SLD] -= lik * D[j + k * SLD];
-                }
+                // uniform trip count across the warp (no divergent inner loops)
+                const double lik = lane < nb ? D[lane + k * SLD] : 0.0;
+                for (int j = k + 1; j < nb; ++j)
+                    if (lane >= j && lane < nb) D[lane + j * SLD] -= lik * D[j + k * SLD];
                 __syncwarp();
             }
         }
@@ -764,14 +802,20 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
         A[i + (long)j * lda] = i >= j ? S[i + j * SLD] : 0.0;
     }
     if (inv) {
-        // X = L^{-1}: thread j solves L x = e_j from row j down
+        // X = L^{-1}: thread j solves L x = e_j.  Every thread walks the same
+        // rows i and terms k (X[k][j] = 0 above the diagonal), so the warp never
+        // diverges and L[i][k] is a broadcast read.
         if (tid < n) {
             const int j = tid;
-            for (int i = 0; i < j; ++i) X[i + j * SLD] = 0.0;
+            for (int i = 0; i < n; ++i) X[i + j * SLD] = 0.0;
             X[j + j * SLD] = 1.0 / S[j + j * SLD];
-            for (int i = j + 1; i < n; ++i) {
+        }
+        __syncthreads();
+        if (tid < n) {
+            const int j = tid;
+            for (int i = 1; i < n; ++i) {
                 double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-                int k = j;
+                int k = 0;
                 for (; k + 3 < i; k += 4) {
                     s0 += S[i + k * SLD] * X[k + j * SLD];
                     s1 += S[i + (k + 1) * SLD] * X[k + 1 + j * SLD];
@@ -779,7 +823,8 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
                     s3 += S[i + (k + 3) * SLD] * X[k + 3 + j * SLD];
                 }
                 for (; k < i; ++k) s0 += S[i + k * SLD] * X[k + j * SLD];
-                X[i + j * SLD] = -((s0 + s1) + (s2 + s3)) / S[i + i * SLD];
+                const double v = -((s0 + s1) + (s2 + s3)) / S[i + i * SLD];
+                if (i > j) X[i + j * SLD] = v;
             }
         }
         __syncthreads();

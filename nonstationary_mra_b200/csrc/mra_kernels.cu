@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
         T* V = t.ws + blockIdx.x * t.ws_stride;   // r x r
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r);
+            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r, sm);
             __syncthreads();
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             gemm<T, false, false>(r, r, r, (T)1, t.Pinv + a * rr, r, V, r, (T)0, Ui + (long)j * r, mr, sm);
         }
         T* Li = t.Lprior + i * rr;
-        fill_cov<T>(g, t.pts, i * r, r, i * r, r, true, Li, r);
+        fill_cov<T>(g, t.pts, i * r, r, i * r, r, true, Li, r, sm);
         __syncthreads();
         if (m > 0) gemm<T, true, false>(r, r, (int)mr, (T)-1, Ui, mr, Ui, mr, (T)1, Li, r, sm);
         double ld = 0.0;
@@ -314,7 +314,7 @@ __device__ __noinline__ double finest_children_grouped(const Geom& g, const DevT
         const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
         T* Sg = ws;                      // np x np conditional covariance of the group
         T* Binv = ws + (long)np * np;    // np x np block-diagonal L_Sigma^{-1}
-        fill_cov<T>(g, t.pts, t.obs0 + lo, np, t.obs0 + lo, np, true, Sg, np);
+        fill_cov<T>(g, t.pts, t.obs0 + lo, np, t.obs0 + lo, np, true, Sg, np, sm);
         for (int e = tid; e < np * np; e += kThreads) Binv[e] = 0.0;
         __syncthreads();
         gemm<T, true, false>(np, np, (int)Lr, (T)-1, t.Ufin + lo * Lr, Lr, t.Ufin + lo * Lr, Lr, (T)1, Sg, np, sm);
@@ -340,10 +340,9 @@ __device__ __noinline__ double finest_children_grouped(const Geom& g, const DevT
                     if (lane == k) Sw[k + k * LD] = sq;
                     if (lane > k && lane < n) Sw[lane + k * LD] *= 1.0 / sq;
                     __syncwarp();
-                    if (lane > k && lane < n) {
-                        const double lik = Sw[lane + k * LD];
-                        for (int j = k + 1; j <= lane; ++j) Sw[lane + j * LD] -= lik * Sw[j + k * LD];
-                    }
+                    const double lik = lane < n ? Sw[lane + k * LD] : 0.0;
+                    for (int j = k + 1; j < n; ++j)  // uniform trip count across the warp
+                        if (lane >= j && lane < n) Sw[lane + j * LD] -= lik * Sw[j + k * LD];
                     __syncwarp();
                 }
                 T* Lc = t.Lsig + t.lsig_off[c];
@@ -364,14 +363,24 @@ __device__ __noinline__ double finest_children_grouped(const Geom& g, const DevT
                 double yy = lane < n ? xl * xl : 0.0;
                 for (int o = 16; o > 0; o >>= 1) yy += __shfl_xor_sync(0xffffffffu, yy, o);
                 // column j of L_Sigma^{-1} by lane j, into the child's diagonal block
-                if (lane < n) {
+                {
+                    // lanes walk the same rows and terms (X[k] = 0 above the
+                    // diagonal): no divergence, broadcast reads of L
                     const int j = lane;
-                    T* X = Binv + q0 + (long)(q0 + j) * np;  // X[i] = row q0+i of column q0+j
-                    X[j] = 1.0 / Sw[j + j * LD];
-                    for (int i = j + 1; i < n; ++i) {
+                    double xs[kChildMax];  // column j of the inverse, in registers
+#pragma unroll
+                    for (int i = 0; i < kChildMax; ++i) xs[i] = 0.0;
+                    double* col = Binv + q0 + (long)(q0 + (j < n ? j : 0)) * np;
+                    for (int i = 0; i < n; ++i) {
                         double v = 0.0;
-                        for (int k = j; k < i; ++k) v += Sw[i + k * LD] * X[k];
-                        X[i] = -v / Sw[i + i * LD];
+#pragma unroll
+                        for (int k = 0; k < kChildMax; ++k)
+                            if (k < i) v += Sw[i + k * LD] * xs[k];
+                        const double xi = i == j ? 1.0 / Sw[i + i * LD] : (i > j ? -v / Sw[i + i * LD] : 0.0);
+#pragma unroll
+                        for (int k = 0; k < kChildMax; ++k)
+                            if (k == i) xs[k] = xi;
+                        if (j < n && i >= j) col[i] = xi;
                     }
                 }
                 part = yy + 2.0 * ldp;
@@ -431,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
             for (int j = 0; j < L; ++j) {
                 const long a = anc[j];
                 T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
-                fill_cov<T>(g, t.pts, a * r, r, t.obs0 + lo, np, false, V, Lr);
+                fill_cov<T>(g, t.pts, a * r, r, t.obs0 + lo, np, false, V, Lr, sm);
                 __syncthreads();
                 if (j > 0) {
                     const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
@@ -449,7 +458,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
                 const int n = (int)(t.obs_off[c + 1] - o0);
                 if (n == 0) continue;
                 T* S = t.Lsig + t.lsig_off[c];
-                fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n);
+                fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n, sm);
                 __syncthreads();
                 gemm<T, true, false>(n, n, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, t.Ufin + o0 * Lr, Lr, (T)1, S, n,
                                      sm);
@@ -602,7 +611,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
         for (int j = 0; j < L; ++j) {
             const long a = anc[j];
             T* Cj = Bt + (long)j * r;
-            fill_cov<T>(g, t.pts, a * r, r, t.pred0 + p0, np, false, Cj, Lr);
+            fill_cov<T>(g, t.pts, a * r, r, t.pred0 + p0, np, false, Cj, Lr, sm);
             __syncthreads();
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
@@ -630,7 +639,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
         __syncthreads();
         if (n > 0) {
             T* Pc = t.Pc + t.pc_off[k];  // n x np, ld = n
-            fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.pred0 + p0, np, false, Pc, n);
+            fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.pred0 + p0, np, false, Pc, n, sm);
             __syncthreads();
             gemm<T, true, false>(n, np, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, P, Lr, (T)1, Pc, n, sm);
             trsm_left_lower<T>(n, np, t.Lsig + t.lsig_off[k], n, Pc, n, sm);
