@@ -65,6 +65,7 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-graph", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--fit", action="store_true",
                    help="instead of the log-likelihood line: fit wall-time of the plain optimizer vs the "
                         "surrogate-assisted one (19 nonstationary parameters, c2 layout)")
@@ -360,6 +361,7 @@ def main():
     if not args.no_graph:
         ctx.capture_graph()
         ctx.loglik()
+    tiles, tune_ms = ctx.autotune(1) if not args.no_autotune else (None, None)
 
     def barrier():
         torch.cuda.synchronize()
@@ -453,6 +455,7 @@ def main():
         "config": {"workload": workload_name(cfg), "precision": args.precision, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (whole tree resident in HBM, no flush needed)",
                    "cuda_graph": not args.no_graph, "loglik": ll, "d": d, "n_obs": st.n_obs,
+                   "autotuned_tile_widths": tiles,
                    "setup_seconds": setup_s, "device_gb": stats["bytes_device"] / 1e9,
                    "flop_per_eval": stats["flop_last"],
                    "stage_ms": {k: stats[k] for k in ("ms_fields", "ms_prior", "ms_finest", "ms_posterior")},

@@ -187,6 +187,17 @@ mra_status mra_eval_covariance(const mra_model* m, const mra_theta* theta, const
 mra_status mra_eval_fields(const mra_model* m, const mra_theta* theta, const double* p, uint64_t n,
                            double* out);
 
+/* Autotuner of the FP64 products' tile shapes.  No counterpart in the
+ * reference.  Times `evals` log-likelihood evaluations of this context (after
+ * one warm-up) for each candidate CTA tile width per product-width bucket
+ * (products at most 16, at most 32, and more than 32 columns wide; widths of
+ * 16, 32 or 64 columns over 64 rows) and keeps the fastest for the device.
+ * The choice is per device and shared by every context on it; results are
+ * bitwise the same for every choice (each element is accumulated by one thread
+ * in the same order).  choice_out (3 ints, may be NULL): the widths in units of
+ * 16 columns; ms_out (may be NULL): the best time per evaluation. */
+mra_status mra_autotune(mra_ctx* ctx, int32_t evals, int32_t* choice_out, double* ms_out);
+
 /* Selects the CUDA device that the calling thread's next mra_create uses
  * (one process per GPU: call it with the local rank before mra_create). */
 mra_status mra_set_device(int32_t device);

@@ -120,6 +120,14 @@ class Context:
         check(self._lib.mra_predict(self._h, f64p(mean), f64p(var)), "mra_predict")
         return mean, var
 
+    def autotune(self, evals: int = 2):
+        """Picks the FP64 tile widths by timing this context (mra_autotune);
+        returns (widths per bucket in units of 16 columns, best ms per evaluation)."""
+        ch = (C.c_int32 * 3)()
+        ms = C.c_double()
+        check(self._lib.mra_autotune(self._h, int(evals), ch, C.byref(ms)), "mra_autotune")
+        return list(ch), ms.value
+
     def capture_graph(self):
         check(self._lib.mra_capture_graph(self._h), "mra_capture_graph")
 

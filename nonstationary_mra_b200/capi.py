@@ -90,6 +90,7 @@ SIGNATURES = [
     ("mra_eval_fields", C.c_int, [C.POINTER(mra_model), C.POINTER(mra_theta), _p_f64, C.c_uint64, _p_f64]),
     ("mra_eval_covariance_static", C.c_int, [C.POINTER(mra_model), C.POINTER(mra_theta), C.c_void_p, C.c_uint64,
                                              C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p]),
+    ("mra_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), _p_f64]),
     ("mra_set_device", C.c_int, [C.c_int32]),
     ("mra_timer_start", C.c_int, [C.c_void_p]),
     ("mra_timer_stop", C.c_int, [C.c_void_p, _p_f64]),

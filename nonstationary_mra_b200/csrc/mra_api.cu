@@ -385,10 +385,10 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     }
     t.ws_stride = post_part ? std::max((long)r * c->tf + 2L * c->tf * c->tf, n_slices(M - 1) * rr + (long)(M - 2) * rr + rr) + 64
                             : 64;
-    // prior: V of one conditioning step; finest: the inverse of a child's
+    // prior: C(Q_a, Q_i) of every ancestor (m r x r); finest: the inverse of a child's
     // L_Sigma (n x n, n <= 64), or a whole sibling group's conditional
     // covariance and block-diagonal inverse (2 x 64 x 64)
-    if (prior_part) t.ws_stride = std::max(t.ws_stride, std::max(rr, 2L * 64 * 64) + 64);
+    if (prior_part) t.ws_stride = std::max(t.ws_stride, std::max((long)(M - 2) * rr, 2L * 64 * 64) + 64);
     t.wsd_stride = post_part ? (long)(M - 1) * r + c->tf + 64 : 64;
     if (!post_part) {
         for (int p = 0; p < 2; ++p) aout_sz[p] = wout_sz[p] = F_sz[p] = f_sz[p] = 1;
@@ -804,6 +804,35 @@ mra_status mra_timer_stop(mra_ctx* c, double* ms) {
     float f = 0;
     CU(cudaEventElapsedTime(&f, c->ev[6], c->ev[7]));
     *ms = f;
+    return MRA_OK;
+}
+
+mra_status mra_autotune(mra_ctx* c, int32_t evals, int32_t* choice_out, double* ms_out) {
+    if (!c || evals < 1) return fail(MRA_ERR_ARG, "mra_autotune: NULL context or evals < 1");
+    // candidate FP64 tile widths per product-width bucket (N <= 16, <= 32, wider)
+    static const int cand[][3] = {{1, 2, 4}, {1, 2, 2}, {1, 4, 4}, {2, 2, 4}, {1, 1, 4}, {2, 4, 4}};
+    const int nc = (int)(sizeof(cand) / sizeof(cand[0]));
+    double best = 1e300;
+    int ib = 0;
+    for (int k = 0; k < nc; ++k) {
+        CU(set_gemm_tiles(cand[k]));
+        double d, ll, ms = 0.0;
+        mra_status st = mra_loglik(c, &d, &ll);  // warm-up with this choice
+        if (st != MRA_OK) return st;
+        st = mra_timer_start(c);
+        if (st != MRA_OK) return st;
+        for (int e = 0; e < evals; ++e) {
+            st = mra_loglik(c, &d, &ll);
+            if (st != MRA_OK) return st;
+        }
+        st = mra_timer_stop(c, &ms);
+        if (st != MRA_OK) return st;
+        if (ms < best) best = ms, ib = k;
+    }
+    CU(set_gemm_tiles(cand[ib]));
+    if (choice_out)
+        for (int b = 0; b < 3; ++b) choice_out[b] = cand[ib][b];
+    if (ms_out) *ms_out = best / evals;
     return MRA_OK;
 }
 

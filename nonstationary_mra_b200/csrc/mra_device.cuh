@@ -212,9 +212,12 @@ __device__ __forceinline__ LaSmem<T>& la_smem() {
 // sqrt(s1) sqrt(s2) pre(x) matern(h) with x = 2 b1 b2 / (b1^2 + b2^2) and
 // h = scale sqrt(2 d^2 / (b1^2 + b2^2)): one division, one square root and
 // one exponential per entry.  Ends with a barrier; uses the tile buffers of sm.
+// fill_cov_blocks: nblk blocks of na rows each, block k from the row points
+// starting at a0[k], written to out + k * blk (same columns for every block);
+// `self` applies to block 0 only.
 template <typename T>
-__device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
-                                      T* out, long ld, LaSmem<T>& sm) {
+__device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, const long* a0, int nblk, int na,
+                                             long b0, int nb, bool self, T* out, long ld, long blk, LaSmem<T>& sm) {
     constexpr int CH = sizeof(T) == 8 ? 512 : 96;  // columns staged per chunk
     double* sx = reinterpret_cast<double*>(&sm.A[0][0]);
     double* sy = sx + CH;
@@ -222,7 +225,8 @@ __device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0,
     double* ss = sz + CH;
     double* sb = ss + CH;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int rows = na < nt ? na : nt;
+    const int R = nblk * na;  // all rows of all blocks
+    const int rows = R < nt ? R : nt;
     const int cols = nt / rows;
     const bool worker = tid < rows * cols;
     const int tr = tid % rows, tq = tid / rows;
@@ -240,8 +244,10 @@ __device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0,
         }
         __syncthreads();
         if (!worker) continue;
-        for (int t = tr; t < na; t += rows) {
-            const long ia = a0 + t;
+        for (int tt = tr; tt < R; tt += rows) {
+            const int kb = tt / na, t = tt - kb * na;
+            const long ia = a0[kb] + t;
+            T* ob = out + kb * blk;
             const Pt pa = P.pt(ia);
             const double sa = P.s2[ia], ba = P.beta[ia];
             const double ssa = sqrt(sa), ba2 = ba * ba;
@@ -249,7 +255,7 @@ __device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0,
             for (int q = tq; q < qn; q += cols) {
                 const int qq = q0 + q;
                 T v;
-                if (self && t == qq) {
+                if (self && kb == 0 && t == qq) {
                     v = (T)(sa + P.t2[ia]);
                 } else if (fast) {
                     const double dx = sx[q] - pa.c0, dy = sy[q] - pa.c1, dz = sz[q] - pa.c2;
@@ -265,11 +271,17 @@ __device__ __noinline__ void fill_cov(const Geom& g, const PointSet& P, long a0,
                     v = (T)cov_entry_f(g, pa, (float)sa, (float)ba, Pt{sx[q], sy[q], sz[q]}, (float)ss[q],
                                        (float)sb[q]);
                 }
-                out[t + (long)qq * ld] = v;
+                ob[t + (long)qq * ld] = v;
             }
         }
     }
     __syncthreads();
+}
+
+template <typename T>
+__device__ inline void fill_cov(const Geom& g, const PointSet& P, long a0, int na, long b0, int nb, bool self,
+                                T* out, long ld, LaSmem<T>& sm) {
+    fill_cov_blocks<T>(g, P, &a0, 1, na, b0, nb, self, out, ld, 0, sm);
 }
 
 // ---- FP64: warp tile (8 NW) rows x 16 columns --------------------------------
@@ -513,12 +525,24 @@ __device__ inline void gemm_f32(int M, int N, int K, float alpha, const float* A
 // C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N, column-major,
 // any leading dimensions; A and B in global memory.  beta == 0 never reads C.
 // Ends with a barrier.
-template <typename T, bool TA, bool TB>
+// FP64 tile width (NW) per product-width bucket (N <= 16, N <= 32, wider),
+// chosen per device by the autotuner (mra_autotune); {1, 2, 4} by default.
+// The choice changes only how output tiles are spread over warps: every
+// element is accumulated by one thread in the same K order, so results are
+// bitwise the same whatever the choice.
+__constant__ int c_gemm_nw[3] = {1, 2, 4};
+
+// ONE_TILE: the product must be computed as one column tile (N <= 64) --
+// required when C aliases A (an in-place product C = C X): each row tile then
+// reads all of its rows before writing them, whereas a second column tile
+// would read columns the first one has already overwritten.
+template <typename T, bool TA, bool TB, bool ONE_TILE = false>
 __device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta, T* C,
                             long ldc, LaSmem<T>& sm) {
     if constexpr (sizeof(T) == 8) {
-        if (N <= 16) gemm_f64<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
-        else if (N <= 32) gemm_f64<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        const int nw = ONE_TILE ? (N <= 16 ? 1 : (N <= 32 ? 2 : 4)) : c_gemm_nw[N <= 16 ? 0 : (N <= 32 ? 1 : 2)];
+        if (nw == 1) gemm_f64<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        else if (nw == 2) gemm_f64<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
         else gemm_f64<TA, TB, 4>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
     } else {
         gemm_f32<TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);

@@ -109,11 +109,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             }
         }
         T* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
-        T* V = t.ws + blockIdx.x * t.ws_stride;   // r x r
+        // C(Q_{a_j}, Q_i) for every ancestor at once: m blocks of r x r
+        T* Cs = t.ws + blockIdx.x * t.ws_stride;
+        long aoff[kMaxLevels];
+        for (int j = 0; j < m; ++j) aoff[j] = anc[j] * r;
+        if (m > 0) fill_cov_blocks<T>(g, t.pts, aoff, m, r, i * r, r, false, Cs, r, rr, sm);
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r, sm);
-            __syncthreads();
+            T* V = Cs + (long)j * rr;
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm);
@@ -394,7 +397,8 @@ __device__ __noinline__ double finest_children_grouped(const Geom& g, const DevT
         if (tid == 0)
             for (int k = 0; k < kThreads / 32; ++k) tot += sm.red[k];
         __syncthreads();
-        gemm<T, false, true>((int)Lr, np, np, (T)1, t.Bhat + lo * Lr, Lr, Binv, np, (T)0, t.Bhat + lo * Lr, Lr, sm);
+        gemm<T, false, true, true>((int)Lr, np, np, (T)1, t.Bhat + lo * Lr, Lr, Binv, np, (T)0, t.Bhat + lo * Lr, Lr,
+                                   sm);
         return tot;
     }
 }
@@ -437,11 +441,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
         if (np > 0) {
             T* Uf = t.Ufin + lo * Lr;  // (L r) x np, ld = L r
             T* Bh = t.Bhat + lo * Lr;
+            // C(Q_{a_j}, S) for every ancestor at once, into the blocks of B^
+            long aoff[kMaxLevels];
+            for (int j = 0; j < L; ++j) aoff[j] = anc[j] * r;
+            fill_cov_blocks<T>(g, t.pts, aoff, L, r, t.obs0 + lo, np, false, Bh, Lr, r, sm);
             for (int j = 0; j < L; ++j) {
                 const long a = anc[j];
                 T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
-                fill_cov<T>(g, t.pts, a * r, r, t.obs0 + lo, np, false, V, Lr, sm);
-                __syncthreads();
                 if (j > 0) {
                     const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                     gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, Uf, Lr, (T)1, V, Lr, sm);
@@ -473,8 +479,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
                 if (small) {
                     // B^ = V L_Sigma^{-T}, in place: each 64-row tile of the product
                     // reads exactly the rows it then writes
-                    gemm<T, false, true>((int)Lr, n, n, (T)1, t.Bhat + o0 * Lr, Lr, Sinv, n, (T)0, t.Bhat + o0 * Lr,
-                                         Lr, sm);
+                    gemm<T, false, true, true>((int)Lr, n, n, (T)1, t.Bhat + o0 * Lr, Lr, Sinv, n, (T)0,
+                                               t.Bhat + o0 * Lr, Lr, sm);
                 } else {
                     trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
                 }
@@ -810,6 +816,8 @@ static cudaError_t prepare_type() {
     set((const void*)k_sample<T>);
     return e;
 }
+
+cudaError_t set_gemm_tiles(const int nw[3]) { return cudaMemcpyToSymbol(c_gemm_nw, nw, 3 * sizeof(int)); }
 
 cudaError_t prepare_kernels() {
     cudaError_t e = prepare_type<double>();

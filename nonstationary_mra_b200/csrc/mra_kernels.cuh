@@ -99,6 +99,10 @@ void set_last_error(const char* msg);
 // device; call before the first launch (and before any stream capture).
 cudaError_t prepare_kernels();
 
+// FP64 GEMM tile width per product-width bucket on the current device
+// (c_gemm_nw in mra_device.cuh).
+cudaError_t set_gemm_tiles(const int nw[3]);
+
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
 template <typename T>

@@ -162,6 +162,15 @@ def test_graph_replay_and_theta_updates():
     ctx.close()
 
 
+def test_autotune_keeps_results_bitwise():
+    st, md = random_case(12, 4, 4, 16, 1500, 10, clustered=True)
+    ctx, (d0, _) = run_loglik(st, md)
+    choice, ms = ctx.autotune(1)
+    assert len(choice) == 3 and all(c in (1, 2, 4) for c in choice) and ms > 0
+    assert ctx.loglik()[0] == d0
+    ctx.close()
+
+
 def test_deterministic():
     st, md = random_case(9, 4, 3, 16, 1200, 10, clustered=True)
     ctx, (d0, _) = run_loglik(st, md)
