@@ -385,10 +385,10 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     }
     t.ws_stride = post_part ? std::max((long)r * c->tf + 2L * c->tf * c->tf, n_slices(M - 1) * rr + (long)(M - 2) * rr + rr) + 64
                             : 64;
-    // prior: C(Q_a, Q_i) of every ancestor (m r x r); finest: the inverse of a child's
-    // L_Sigma (n x n, n <= 64), or a whole sibling group's conditional
+    // prior: V of one conditioning step (r x r); finest: the inverse of a
+    // child's L_Sigma (n x n, n <= 64), or a whole sibling group's conditional
     // covariance and block-diagonal inverse (2 x 64 x 64)
-    if (prior_part) t.ws_stride = std::max(t.ws_stride, std::max((long)(M - 2) * rr, 2L * 64 * 64) + 64);
+    if (prior_part) t.ws_stride = std::max(t.ws_stride, std::max(rr, 2L * 64 * 64) + 64);
     t.wsd_stride = post_part ? (long)(M - 1) * r + c->tf + 64 : 64;
     if (!post_part) {
         for (int p = 0; p < 2; ++p) aout_sz[p] = wout_sz[p] = F_sz[p] = f_sz[p] = 1;

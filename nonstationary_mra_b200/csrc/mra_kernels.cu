@@ -109,14 +109,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             }
         }
         T* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
-        // C(Q_{a_j}, Q_i) for every ancestor at once: m blocks of r x r
-        T* Cs = t.ws + blockIdx.x * t.ws_stride;
-        long aoff[kMaxLevels];
-        for (int j = 0; j < m; ++j) aoff[j] = anc[j] * r;
-        if (m > 0) fill_cov_blocks<T>(g, t.pts, aoff, m, r, i * r, r, false, Cs, r, rr, sm);
+        // one r x r scratch per CTA (stays in L2; a scratch for all m ancestors at
+        // once doubled the DRAM traffic of the launch at no gain in time)
+        T* V = t.ws + blockIdx.x * t.ws_stride;
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            T* V = Cs + (long)j * rr;
+            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r, sm);
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm);
