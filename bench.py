@@ -70,6 +70,9 @@ def parse_args():
                    help="instead of the log-likelihood line: fit wall-time of the plain optimizer vs the "
                         "surrogate-assisted one (19 nonstationary parameters, c2 layout)")
     p.add_argument("--fit-evals", type=int, default=2000)
+    p.add_argument("--sweep", action="store_true",
+                   help="instead of the log-likelihood line: the scaling sweep n in {1M, 2M, 4M} x M in "
+                        "{10, 11, 12} x r in {32, 64, 128} (one JSON line per case)")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -322,6 +325,60 @@ def fit_arm(args):
     print(json.dumps(line))
 
 
+def sweep_arm(args):
+    """Scaling sweep (uniform locations, nu = 1/2, J = 4, 4 observations per finest
+    region): per case the FP64 log-likelihood and log-likelihood + prediction
+    (16,384 points) times, the device memory high-water and the dominant
+    launch's FP64 tensor throughput; cases that do not fit in device memory are
+    reported as such (the library's allocation fails cleanly)."""
+    import torch
+    from nonstationary_mra_b200 import api, capi, synth
+    cases = [(1 << 20, 10), (1 << 21, 11), (1 << 22, 12)]
+    peak = fp64_peak_tflops()
+    for n, M in cases:
+        for r in (32, 64, 128):
+            cfg = synth.Config(f"sweep-{n}-{M}-{r}", n, M, 4, r, 1, 16384, "uniform", 0.3, 5)
+            line = {"metric": "MRA loglik evals/sec (scaling sweep)", "unit": "evals/s", "n": n, "M": M, "r": r,
+                    "workload": workload_name(cfg)}
+            try:
+                xy, pred, theta, md, st = make_problem(cfg, with_pred=True)
+                ctx = api.Context(st, md)
+            except capi.MRAError as exc:
+                line.update(value=None, infeasible=str(exc)[:200])
+                print(json.dumps(line), flush=True)
+                continue
+            try:
+                y = draw_values(ctx, st, cfg.seed + 7)
+                ctx.set_obs_values(y)
+                ctx.set_theta()
+                for _ in range(max(args.warmup, 1)):
+                    ctx.loglik()
+                ctx.capture_graph()
+                ctx.loglik()
+                steps = max(args.steps, 1)
+                ctx.timer_start()
+                for _ in range(steps):
+                    _, ll = ctx.loglik()
+                ms = ctx.timer_stop() / steps
+                stats = ctx.stats()
+                dom = max(stats["launches"], key=lambda l: l["ms"])
+                ctx.predict()
+                ctx.timer_start()
+                ctx.predict()
+                ms_pred = ctx.timer_stop()
+                line.update(value=1000.0 / ms, ms_per_eval=ms, loglik=ll, flop_per_eval=stats["flop_last"],
+                            predict_ms=ms_pred, predictions=int(st.n_pred),
+                            device_gb=stats["bytes_device"] / 1e9,
+                            dominant=f"{dom['kernel']}(level {dom['level']})",
+                            dominant_tflops=dom["flop"] / (dom["ms"] * 1e-3) / 1e12, fp64_peak_tflops=peak)
+            except capi.MRAError as exc:
+                line.update(value=None, failed=str(exc)[:200])
+            finally:
+                ctx.close()
+                torch.cuda.empty_cache()
+            print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -329,6 +386,9 @@ def main():
     args = parse_args()
     if args.fit:
         fit_arm(args)
+        return
+    if args.sweep:
+        sweep_arm(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
