@@ -448,12 +448,10 @@ def main():
     ms_e2e = ctx.timer_stop()
     barrier()
 
-    t_max = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms, ms_e2e = t_max.tolist()
-    value = world * args.steps / (ms * 1e-3)
-    e2e = world * args.steps / (ms_e2e * 1e-3)
+    from nonstationary_mra_b200 import replicas
+    ms, ms_e2e = replicas.max_over_ranks([ms, ms_e2e], device="cuda")
+    value = replicas.job_throughput(args.steps, world, ms)
+    e2e = replicas.job_throughput(args.steps, world, ms_e2e)
 
     # roofline of the dominant launch of one evaluation
     launches = stats["launches"]
