@@ -742,78 +742,136 @@ __device__ inline int potrf_blocked(int n, T* A, long lda, LaSmem<T>& sm, double
 }
 
 
-// FP64 Cholesky of an n x n matrix, n <= 64, staged whole in shared memory
-// (column-major, ld 65): unblocked right-looking, two barriers per column,
-// column scaling by the reciprocal of the pivot (LAPACK's dpotf2 order).  The
-// log-determinant is summed over the diagonal in parallel at the end.  With
-// `inv` the inverse of the factor is also formed (column j by thread j,
-// forward substitution against the staged factor) and written to inv.
+// FP64 Cholesky (and optionally the inverse of the factor) of an n x n
+// matrix, n <= 64, staged whole in shared memory (column-major, ld 65),
+// right-looking in 16-wide block columns:
+//  * each 16 x 16 diagonal block is factored by one warp with lane l holding
+//    row l in registers (pivots broadcast by shuffles, 1/sqrt(pivot) by
+//    rsqrt), and the same warp inverts the block (lane l: column l);
+//  * the panel below it is the product of the panel with the block's inverse
+//    (transposed), and the trailing update a rank-16 product, each thread
+//    owning rows tx + 16a / columns ty + 16c of the 16 x 16 thread grid;
+//  * X = L^{-1} is completed block by block away from the diagonal:
+//    X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj.
+// n that is not a multiple of 16 is padded with an identity block.  A
+// non-positive or NaN pivot sets sm.flag (1-based index, first wins) and the
+// factorization goes on with NaNs.  logdet (thread 0) = 2 sum log L_ii.
 constexpr int SLD = 65;
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// One warp: factors the 16 x 16 block of S at (b0, b0) in place and writes its
+// inverse to the same block of X (both with zeros above the diagonal).
+static __device__ __noinline__ void potrf_diag16(double* S, double* X, int b0, LaSmem<double>& sm) {
+    const int l = threadIdx.x & 31;
+    double x[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) x[c] = (l < 16 && c <= l) ? S[(b0 + l) + (b0 + c) * SLD] : 0.0;
+    int bad = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const double d = __shfl_sync(kFullMask, x[k], k);
+        if (!(d > 0.0) && bad == 0) bad = b0 + k + 1;
+        const double r = rsqrt(d);
+        if (l == 0) sm.inv[k] = r;
+        x[k] = l == k ? d * r : (l > k ? x[k] * r : x[k]);
+#pragma unroll
+        for (int j = k + 1; j < 16; ++j) {
+            const double ljk = __shfl_sync(kFullMask, x[k], j);
+            if (l >= j) x[j] = fma(-x[k], ljk, x[j]);
+        }
+    }
+    if (l < 16) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) S[(b0 + l) + (b0 + c) * SLD] = c <= l ? x[c] : 0.0;
+    }
+    if (l == 0 && bad && sm.flag == 0) sm.flag = bad;
+    __syncwarp();
+    double y[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) y[i] = i == l ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        y[k] *= sm.inv[k];
+#pragma unroll
+        for (int i = k + 1; i < 16; ++i) y[i] = fma(-S[(b0 + i) + (b0 + k) * SLD], y[k], y[i]);
+    }
+    if (l < 16) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) X[(b0 + i) + (b0 + l) * SLD] = y[i];
+    }
+}
 
 __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm, double* logdet, double* inv,
                                   long ldinv) {
     const int tid = threadIdx.x;
     double* S = &sm.A[0][0];  // 64 x 65 (fits in the operand tile buffers)
     double* X = &sm.B[0][0];
-    for (int e = tid; e < n * n; e += kThreads) {
-        const int i = e % n, j = e / n;
-        S[i + j * SLD] = A[i + (long)j * lda];
+    const int nbk = (n + 15) >> 4, N = nbk << 4;
+    {
+        // every load issued before the first store (16 columns per thread)
+        const int i = tid & 63, j0 = tid >> 6;
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int j = j0 + 4 * q;
+            v[q] = (i < n && j < n) ? A[i + (long)j * lda] : (i == j ? 1.0 : 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int j = j0 + 4 * q;
+            if (i < N && j < N) S[i + j * SLD] = v[q];
+        }
     }
     if (tid == 0) sm.flag = 0;
     __syncthreads();
     const int tx = tid & 15, ty = tid >> 4;
-    for (int b0 = 0; b0 < n; b0 += NB) {
-        const int nb = min(NB, n - b0);
-        // diagonal block by warp 0, lane i owning row b0+i (right-looking)
-        if (tid < 32) {
-            const int lane = tid;
-            double* D = S + b0 + b0 * SLD;
-            for (int k = 0; k < nb; ++k) {
-                if (lane == 0) {
-                    const double d = D[k + k * SLD];
-                    if (!(d > 0.0) && sm.flag == 0) sm.flag = b0 + k + 1;
-                    const double sq = sqrt(d);
-                    D[k + k * SLD] = sq;
-                    sm.inv[k] = 1.0 / sq;
-                }
-                __syncwarp();
-                if (lane > k && lane < nb) D[lane + k * SLD] *= sm.inv[k];
-                __syncwarp();
-                // uniform trip count across the warp (no divergent inner loops)
-                const double lik = lane < nb ? D[lane + k * SLD] : 0.0;
-                for (int j = k + 1; j < nb; ++j)
-                    if (lane >= j && lane < nb) D[lane + j * SLD] -= lik * D[j + k * SLD];
-                __syncwarp();
-            }
-        }
+    for (int b = 0; b < nbk; ++b) {
+        const int b0 = b << 4;
+        if (tid < 32) potrf_diag16(S, X, b0, sm);
         __syncthreads();
-        if (b0 + nb < n) {
-            // panel: each row below solves x L_d^T = a against the diagonal block
-            for (int i = b0 + nb + tid; i < n; i += kThreads) {
-                double x[NB];
+        const int rest = N - b0 - 16;
+        if (rest > 0) {
+            const int r0 = b0 + 16, na = rest >> 4;
+            // panel: L[i][b0+k] = sum_{c<=k} A[i][b0+c] Y[k][c], Y the block's inverse
+            double v[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-                for (int k = 0; k < NB; ++k) x[k] = k < nb ? S[i + (b0 + k) * SLD] : 0.0;
+            for (int c = 0; c < 16; ++c) {
+                if (c <= ty) {
+                    const double yk = X[(b0 + ty) + (b0 + c) * SLD];
 #pragma unroll
-                for (int k = 0; k < NB; ++k) {
-                    if (k < nb) {
-                        double v = x[k];
-#pragma unroll
-                        for (int c = 0; c < k; ++c) v -= x[c] * S[(b0 + k) + (b0 + c) * SLD];
-                        x[k] = v * sm.inv[k];
-                    }
+                    for (int a = 0; a < 3; ++a)
+                        if (a < na) v[a] = fma(S[(r0 + tx + 16 * a) + (b0 + c) * SLD], yk, v[a]);
                 }
-#pragma unroll
-                for (int k = 0; k < NB; ++k)
-                    if (k < nb) S[i + (b0 + k) * SLD] = x[k];
             }
             __syncthreads();
-            // trailing rank-nb update of the lower triangle
-            for (int j = b0 + nb + ty; j < n; j += 16)
-                for (int i = j + tx; i < n; i += 16) {
-                    double v = 0.0;
-                    for (int c = 0; c < nb; ++c) v += S[i + (b0 + c) * SLD] * S[j + (b0 + c) * SLD];
-                    S[i + j * SLD] -= v;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (a < na) S[(r0 + tx + 16 * a) + (b0 + ty) * SLD] = v[a];
+            __syncthreads();
+            // trailing update of the lower triangle
+            double acc[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int e = 0; e < 3; ++e) acc[a][e] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                double li[3], lj[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    li[a] = a < na ? S[(r0 + tx + 16 * a) + (b0 + k) * SLD] : 0.0;
+                    lj[a] = a < na ? S[(r0 + ty + 16 * a) + (b0 + k) * SLD] : 0.0;
                 }
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int e = 0; e <= a; ++e) acc[a][e] = fma(li[a], lj[e], acc[a][e]);
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int e = 0; e <= a; ++e)
+                    if (a < na && (a > e || tx >= ty)) S[(r0 + tx + 16 * a) + (r0 + ty + 16 * e) * SLD] -= acc[a][e];
             __syncthreads();
         }
     }
@@ -821,41 +879,55 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
     for (int i = tid; i < n; i += kThreads) part += log(S[i + i * SLD]);
     const double sum = cta_sum(part, sm);
     if (tid == 0 && logdet) *logdet = 2.0 * sum;
-    for (int e = tid; e < n * n; e += kThreads) {
-        const int i = e % n, j = e / n;
-        A[i + (long)j * lda] = i >= j ? S[i + j * SLD] : 0.0;
+    {
+        const int i = tid & 63;
+        for (int j = tid >> 6; j < n; j += kThreads / 64)
+            if (i < n) A[i + (long)j * lda] = i >= j ? S[i + j * SLD] : 0.0;
     }
     if (inv) {
-        // X = L^{-1}: thread j solves L x = e_j.  Every thread walks the same
-        // rows i and terms k (X[k][j] = 0 above the diagonal), so the warp never
-        // diverges and L[i][k] is a broadcast read.
-        if (tid < n) {
-            const int j = tid;
-            for (int i = 0; i < n; ++i) X[i + j * SLD] = 0.0;
-            X[j + j * SLD] = 1.0 / S[j + j * SLD];
-        }
-        __syncthreads();
-        if (tid < n) {
-            const int j = tid;
-            for (int i = 1; i < n; ++i) {
-                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-                int k = 0;
-                for (; k + 3 < i; k += 4) {
-                    s0 += S[i + k * SLD] * X[k + j * SLD];
-                    s1 += S[i + (k + 1) * SLD] * X[k + 1 + j * SLD];
-                    s2 += S[i + (k + 2) * SLD] * X[k + 2 + j * SLD];
-                    s3 += S[i + (k + 3) * SLD] * X[k + 3 + j * SLD];
+        // off-diagonal blocks of X by distance dd from the diagonal; thread
+        // (tx, ty) forms element (tx, ty) of each block
+        for (int dd = 1; dd < nbk; ++dd) {
+            const int np = nbk - dd;
+            double v[3];
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                v[u] = 0.0;
+                if (u < np) {
+                    const int row = 16 * (u + dd) + tx, col = 16 * u + ty;
+                    double s[4] = {0.0, 0.0, 0.0, 0.0};
+                    for (int kb = u; kb < u + dd; ++kb) {
+#pragma unroll
+                        for (int c = 0; c < 16; ++c)
+                            s[c & 3] = fma(S[row + (16 * kb + c) * SLD], X[(16 * kb + c) + col * SLD], s[c & 3]);
+                    }
+                    v[u] = (s[0] + s[1]) + (s[2] + s[3]);
                 }
-                for (; k < i; ++k) s0 += S[i + k * SLD] * X[k + j * SLD];
-                const double v = -((s0 + s1) + (s2 + s3)) / S[i + i * SLD];
-                if (i > j) X[i + j * SLD] = v;
             }
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (u < np) X[(16 * (u + dd) + tx) + (16 * u + ty) * SLD] = v[u];
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                if (u < np) {
+                    const int ib = u + dd, row = 16 * ib + tx, col = 16 * u + ty;
+                    double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int c = 0; c < 16; ++c)
+                        if (c <= tx) s[c & 3] = fma(X[row + (16 * ib + c) * SLD], X[(16 * ib + c) + col * SLD], s[c & 3]);
+                    v[u] = -((s[0] + s[1]) + (s[2] + s[3]));
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+                if (u < np) X[(16 * (u + dd) + tx) + (16 * u + ty) * SLD] = v[u];
+            __syncthreads();
         }
-        __syncthreads();
-        for (int e = tid; e < n * n; e += kThreads) {
-            const int i = e % n, j = e / n;
-            inv[i + (long)j * ldinv] = X[i + j * SLD];
-        }
+        const int i = tid & 63;
+        for (int j = tid >> 6; j < n; j += kThreads / 64)
+            if (i < n) inv[i + (long)j * ldinv] = i >= j ? X[i + j * SLD] : 0.0;
     }
     __syncthreads();
     return sm.flag;
