@@ -203,15 +203,99 @@ __device__ __forceinline__ LaSmem<T>& la_smem() {
     return *reinterpret_cast<LaSmem<T>*>(la_dyn_smem);
 }
 
+// ---- branch-free FP64 elementary functions for the covariance entries ----
+// e^{-s} for s >= 0 (s clamped at 700, where the result is below 1e-304):
+// Cody-Waite reduction s = n ln2 + r, |r| <= ln2/2, with ln2 split in a
+// 32-bit head (n * head exact) and a tail; e^{-r} from its Taylor polynomial
+// of degree 13 in Horner form (truncation below 5e-18 relative); 2^{-n} built
+// in the exponent field.  Within 1 ulp of exp(-s) on this range (checked on
+// 4M arguments against the CUDA library).
+__device__ __forceinline__ double exp_neg(double s) {
+    s = fmin(s, 700.0);
+    const double kShift = 6755399441055744.0;  // 1.5 * 2^52: rounds s/ln2 to an integer in the low word
+    const double t = fma(s, 1.4426950408889634, kShift);
+    const double n = t - kShift;
+    double r = fma(-n, 0.6931471803691238, s);
+    r = fma(-n, 1.9082149292705877e-10, r);
+    const double u = -r;
+    double p = 1.6059043836821613e-10;  // 1/13!
+    p = fma(p, u, 2.08767569878681e-09);
+    p = fma(p, u, 2.505210838544172e-08);
+    p = fma(p, u, 2.755731922398589e-07);
+    p = fma(p, u, 2.7557319223985893e-06);
+    p = fma(p, u, 2.48015873015873e-05);
+    p = fma(p, u, 0.0001984126984126984);
+    p = fma(p, u, 0.001388888888888889);
+    p = fma(p, u, 0.008333333333333333);
+    p = fma(p, u, 0.041666666666666664);
+    p = fma(p, u, 0.16666666666666666);
+    p = fma(p, u, 0.5);
+    p = fma(p, u, 1.0);
+    p = fma(p, u, 1.0);
+    return p * __hiloint2double((1023 - __double2loint(t)) << 20, 0);
+}
+
+// 1/s from the PTX approximation refined by one third-order Newton step
+// (y <- y (1 + e + e^2), e = 1 - s y); s positive and normal.
+__device__ __forceinline__ double rcp_nr(double s) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(s));
+    const double e = fma(-s, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+}
+
+// 1/sqrt(x) from the PTX approximation refined by one third-order Newton step
+// (y <- y (1 + e/2 + 3e^2/8), e = 1 - x y^2); x positive and normal.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y;
+    asm("rsqrt.approx.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
+// One row point against the staged column points q_begin, q_begin + q_step,
+// ... < q_end (straight-line distance, nonstationary): writes ob[(qoff + q) ld].
+// NU: 1 exponential, 3 Matern 3/2; PREF: 0 prefactor x^1.5, 1 prefactor x.
+// Entry: sqrt(s1 s2) pre(x) matern(h), x = 2 b1 b2 / (b1^2 + b2^2),
+// h = scale sqrt(2 d^2 / (b1^2 + b2^2)).  Every parameter is in registers so
+// the loop carries no reloads; one reciprocal, one inverse square root and
+// one exponential per entry, none with a branch.
+template <typename T, int NU, int PREF>
+__device__ __noinline__ void fill_row_fast(const double* __restrict__ sx, const double* __restrict__ sy,
+                                           const double* __restrict__ sz, const double* __restrict__ ss,
+                                           const double* __restrict__ sb, const double* __restrict__ sb2, double pc0,
+                                           double pc1, double pc2, double ssa, double ba, double hs, int q_begin,
+                                           int q_end, int q_step, int qoff, T* __restrict__ ob, long ld) {
+    const double ba2 = ba * ba, c2 = 2.0 * ba * ssa;
+#pragma unroll 4
+    for (int q = q_begin; q < q_end; q += q_step) {
+        const double dx = sx[q] - pc0, dy = sy[q] - pc1, dz = sz[q] - pc2;
+        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        const double ibms = rcp_nr(ba2 + sb2[q]);  // 1 / (b1^2 + b2^2)
+        const double u = 2.0 * d2 * ibms;
+        const double h = u > 1e-300 ? hs * (u * rsqrt_nr(u)) : 0.0;
+        const double em = exp_neg(h);
+        const double m = NU == 3 ? (1.0 + h) * em : em;
+        double v;
+        if (PREF == 1) {
+            v = (c2 * ss[q]) * (sb[q] * ibms) * m;
+        } else {
+            const double x = 2.0 * ba * sb[q] * ibms;
+            v = (ssa * ss[q]) * (x * sqrt(x)) * m;
+        }
+        ob[(long)(qoff + q) * ld] = (T)v;
+    }
+}
+
 // out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
 // diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
-// The column points (coordinates, sqrt(sigma^2), beta) are staged in shared
-// memory in chunks, each thread keeps one row point in registers and walks
-// columns strided by the number of row groups (consecutive threads write
-// consecutive rows).  For the straight-line nonstationary case the entry is
-// sqrt(s1) sqrt(s2) pre(x) matern(h) with x = 2 b1 b2 / (b1^2 + b2^2) and
-// h = scale sqrt(2 d^2 / (b1^2 + b2^2)): one division, one square root and
-// one exponential per entry.  Ends with a barrier; uses the tile buffers of sm.
+// The column points (coordinates, sqrt(sigma^2), beta, beta^2) are staged in
+// shared memory in chunks, each thread keeps one row point in registers and
+// walks columns strided by the number of row groups (consecutive threads
+// write consecutive rows).  The straight-line nonstationary FP64 case with
+// the prefactor exponents 1.5 or 1 goes through fill_row_fast; the others
+// evaluate cov_entry / cov_entry_f per entry.  Ends with a barrier; uses the
+// tile buffers of sm.
 // fill_cov_blocks: nblk blocks of na rows each, block k from the row points
 // starting at a0[k], written to out + k * blk (same columns for every block);
 // `self` applies to block 0 only.
@@ -224,13 +308,16 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
     double* sz = sy + CH;
     double* ss = sz + CH;
     double* sb = ss + CH;
+    double* sb2 = sb + CH;  // FP64 fast path only (6 CH doubles fit the FP64 tile buffers)
     const int tid = threadIdx.x, nt = blockDim.x;
     const int R = nblk * na;  // all rows of all blocks
     const int rows = R < nt ? R : nt;
     const int cols = nt / rows;
     const bool worker = tid < rows * cols;
     const int tr = tid % rows, tq = tid / rows;
-    const bool fast = sizeof(T) == 8 && g.nonstat && g.distance != 1;
+    const int nu = g.nu_x2, pk = g.pref_kind;
+    const bool fast = sizeof(T) == 8 && g.nonstat && g.distance != 1 && pk != 2;
+    const double hs = g.dist_scale * (nu == 3 ? 1.7320508075688772 : 1.0);
     for (int q0 = 0; q0 < nb; q0 += CH) {
         const int qn = nb - q0 < CH ? nb - q0 : CH;
         __syncthreads();
@@ -240,31 +327,44 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
             sy[e] = P.c1[ib];
             sz[e] = P.c2[ib];
             ss[e] = fast ? sqrt(P.s2[ib]) : P.s2[ib];
-            sb[e] = P.beta[ib];
+            const double bb = P.beta[ib];
+            sb[e] = bb;
+            if (fast) sb2[e] = bb * bb;
         }
         __syncthreads();
         if (!worker) continue;
         for (int tt = tr; tt < R; tt += rows) {
             const int kb = tt / na, t = tt - kb * na;
             const long ia = a0[kb] + t;
+            if (fast) {
+                T* ob = out + kb * blk + t;
+                const double pc0 = P.c0[ia], pc1 = P.c1[ia], pc2 = P.c2[ia];
+                const double sa = P.s2[ia], ba = P.beta[ia];
+                const double ssa = sqrt(sa);
+                if (nu == 3 && pk == 1)
+                    fill_row_fast<T, 3, 1>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                else if (nu == 3)
+                    fill_row_fast<T, 3, 0>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                else if (pk == 1)
+                    fill_row_fast<T, 1, 1>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                else
+                    fill_row_fast<T, 1, 0>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                // the diagonal of a self block, whose entry this thread has just written
+                if (self && kb == 0) {
+                    const int qd = t - q0;
+                    if (qd >= tq && qd < qn && (qd - tq) % cols == 0) ob[(long)t * ld] = (T)(sa + P.t2[ia]);
+                }
+                continue;
+            }
             T* ob = out + kb * blk;
             const Pt pa = P.pt(ia);
             const double sa = P.s2[ia], ba = P.beta[ia];
-            const double ssa = sqrt(sa), ba2 = ba * ba;
 #pragma unroll 4
             for (int q = tq; q < qn; q += cols) {
                 const int qq = q0 + q;
                 T v;
                 if (self && kb == 0 && t == qq) {
                     v = (T)(sa + P.t2[ia]);
-                } else if (fast) {
-                    const double dx = sx[q] - pa.c0, dy = sy[q] - pa.c1, dz = sz[q] - pa.c2;
-                    const double d2 = dx * dx + dy * dy + dz * dz;
-                    const double bb = sb[q];
-                    const double ibms = 2.0 / (ba2 + bb * bb);
-                    const double x = (ba * bb) * ibms;
-                    const double pre = g.pref_kind == 0 ? x * sqrt(x) : (g.pref_kind == 1 ? x : pow(x, g.pref_exp));
-                    v = (T)(ssa * ss[q] * pre * matern(g.nu_x2, g.dist_scale * sqrt(d2 * ibms)));
                 } else if (sizeof(T) == 8) {
                     v = (T)cov_entry(g, pa, sa, ba, Pt{sx[q], sy[q], sz[q]}, ss[q], sb[q]);
                 } else {

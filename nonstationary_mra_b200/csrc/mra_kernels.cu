@@ -261,19 +261,22 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
         for (int tt = 0; tt < r; ++tt) s += (double)Gi[tt + x * r] * v[tt];
         wo[x] = wagg[x] - s;
     }
+    // A_out(j, j..m-1) = A(j, j..m-1) - G_j^T G_{j..m-1}: both slice rows are
+    // contiguous r x r blocks, one copy and one product per j
     T* ao = t.aout[m & 1] + loc * n_slices(m) * rr;
     for (int j = 0; j < m; ++j) {
-        for (int k = j; k < m; ++k) {
-            T* dst = ao + slice_index(m, j, k) * rr;
-            const T* src = Aagg + slice_index(m + 1, j, k) * rr;
-            for (long e = threadIdx.x; e < rr; e += kThreads) dst[e] = src[e];
-            __syncthreads();
-            gemm<T, true, false>(r, r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)k * rr, r, (T)1, dst, r, sm);
-        }
+        T* dst = ao + slice_index(m, j, j) * rr;
+        const T* src = Aagg + slice_index(m + 1, j, j) * rr;
+        const long cnt = (long)(m - j) * rr;
+        for (long e = threadIdx.x; e < cnt; e += kThreads) dst[e] = src[e];
+        __syncthreads();
+        gemm<T, true, false>(r, (m - j) * r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)j * rr, r, (T)1, dst, r, sm);
     }
 }
 
 // Aagg/wagg += the (A~, w~) of factored rows F (n x (m+1) r, row stride ldF), f.
+// The slices (j, j..m) of A~ are contiguous r x r blocks, so block row j is
+// one product F_j^T F_{j..m} (r x (m+1-j) r).
 template <typename T>
 __device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* F, long ldF, const double* f, T* Aagg,
                                     double* wagg, LaSmem<T>& sm) {
@@ -281,9 +284,8 @@ __device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
     if (n == 0) return;
     for (int j = 0; j <= m; ++j)
-        for (int k = j; k <= m; ++k)
-            gemm<T, false, true>(r, r, n, (T)1, F + (long)j * r, ldF, F + (long)k * r, ldF, (T)1,
-                                 Aagg + slice_index(m + 1, j, k) * rr, r, sm);
+        gemm<T, false, true>(r, (m + 1 - j) * r, n, (T)1, F + (long)j * r, ldF, F + (long)j * r, ldF, (T)1,
+                             Aagg + slice_index(m + 1, j, j) * rr, r, sm);
     for (long x = threadIdx.x; x < mr1; x += kThreads) {
         double s = 0.0;
         for (int q = 0; q < n; ++q) s += (double)F[(long)q * ldF + x] * f[q];
@@ -569,9 +571,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
             for (int cc = 1; cc <= t.J; ++cc) {
                 const long c = i * t.J + cc;
                 if (t.factored[c]) {
+                    // factored children with adjacent rows are accumulated together
                     const long lo = t.sub_lo[c];
-                    accumulate_factored<T>(t, m, (int)(t.sub_hi[c] - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg,
-                                           sm);
+                    long hi = t.sub_hi[c], cl = c;
+                    while (cc < t.J && t.factored[cl + 1] && t.sub_lo[cl + 1] == hi) {
+                        ++cc;
+                        ++cl;
+                        hi = t.sub_hi[cl];
+                    }
+                    accumulate_factored<T>(t, m, (int)(hi - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg, sm);
                 } else {
                     const long cl = c - s1;
                     for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] += ain[cl * ns_in * rr + e];
