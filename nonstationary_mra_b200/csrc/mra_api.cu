@@ -368,6 +368,7 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     t.obs_off = idx[0]; t.pred_off = idx[1]; t.fin_anc = idx[2]; t.fin_order = idx[3]; t.lsig_off = idx[4];
     t.pc_off = idx[5]; t.child_lo = idx[6]; t.child_hi = idx[7]; t.par_order = idx[8]; t.sub_lo = idx[9];
     t.sub_hi = idx[10];
+    t.n_fin_items = (long)h.par_order.size();
     // sizes of the level-parity buffers
     size_t aout_sz[2] = {1, 1}, wout_sz[2] = {1, 1}, F_sz[2] = {1, 1}, f_sz[2] = {1, 1};
     for (int m = 1; m <= M - 2; ++m) {
@@ -588,13 +589,40 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         }
     }
     for (long i = 0; i < n_int; ++i) h.factored[i] = (h.sub_hi[i] - h.sub_lo[i]) <= c->tf ? 1 : 0;
-    h.par_order.assign(cnt2, 0);
-    for (long q = 0; q < cnt2; ++q) h.par_order[q] = q;
-    std::stable_sort(h.par_order.begin(), h.par_order.end(), [&](int64_t a, int64_t b) {
-        double na = (double)(h.sub_hi[lvl2 + a] - h.sub_lo[lvl2 + a]);
-        double nb = (double)(h.sub_hi[lvl2 + b] - h.sub_lo[lvl2 + b]);
-        return na * (na + 64.0 * L) > nb * (nb + 64.0 * L);
-    });
+    // work items of the finest kernel: a level M-3 region with its J sibling
+    // groups when it holds at most 64 J observations (conditioning shared by
+    // the groups), else each of its groups alone (load balance); for M = 2 the
+    // single level-0 group.  Most expensive first.
+    {
+        const long n_units = M >= 3 ? level_count(J, M - 3) : 0;
+        const long lvl3 = M >= 3 ? level_start(J, M - 3) : 0;
+        auto group_cost = [&](long gl) {
+            const double n = (double)(h.sub_hi[lvl2 + gl] - h.sub_lo[lvl2 + gl]);
+            return n * (n + 64.0 * L);
+        };
+        std::vector<std::pair<double, int64_t>> items;
+        if (M >= 3) {
+            for (long u = 0; u < n_units; ++u) {
+                const long nu = h.sub_hi[lvl3 + u] - h.sub_lo[lvl3 + u];
+                if (nu <= 64L * J) {
+                    double c = 0.0;
+                    for (long gl = u * J; gl < u * J + J; ++gl) c += group_cost(gl);
+                    items.push_back({c, (int64_t)u});
+                } else {
+                    for (long gl = u * J; gl < u * J + J; ++gl)
+                        items.push_back({group_cost(gl), (int64_t)(n_units + gl)});
+                }
+            }
+        } else {
+            items.push_back({group_cost(0), 0});
+        }
+        std::stable_sort(items.begin(), items.end(),
+                         [](const std::pair<double, int64_t>& x, const std::pair<double, int64_t>& y) {
+                             return x.first > y.first;
+                         });
+        h.par_order.resize(items.size());
+        for (size_t q = 0; q < items.size(); ++q) h.par_order[q] = items[q].second;
+    }
     int64_t u_total = 0;
     for (int mm = 0; mm <= M - 2; ++mm) u_total += level_count(J, mm) * (int64_t)mm * r * r;
 

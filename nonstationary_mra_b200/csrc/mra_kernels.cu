@@ -7,9 +7,11 @@
 //                       prediction point (class_nonstationary_covariance.cpp:479-573)
 //   k_prior_level(m)    levels 0..M-2, one CTA per region: U_{i,j} = L_{a_j}^{-1} V_j,
 //                       L_i = chol(K_i)   (class_approximation.cpp:46-50,84-169)
-//   k_finest_group      one CTA per level M-2 region, its finest children as one
-//                       sibling group: conditioning of all their observations on
-//                       the shared ancestors, then per child Sigma, L_Sigma, y~,
+//   k_finest_group      one CTA per level M-3 region: conditioning of all its
+//                       observations on the shared ancestors (levels 0..M-3),
+//                       then per level M-2 child (a sibling group of finest
+//                       regions) the level M-2 step and per finest region
+//                       Sigma, L_Sigma, y~,
 //                       B^ and the log-lik terms
 //                       (...-loop-regions-at-finest-level-in-prior.cpp:90-269),
 //                       then the level M-2 posterior of the parent
@@ -404,116 +406,145 @@ __device__ __noinline__ double finest_children_grouped(const Geom& g, const DevT
 }
 
 // ---------------------------------------------------------------------------
-// a7/a8 (+ a9 at level M-2): finest level, one CTA per sibling group
+// a7/a8 (+ a9 at level M-2): finest level, one CTA per level M-3 region
 // ---------------------------------------------------------------------------
+// A work item is either a unit -- a level M-3 region with its J level M-2
+// children (sibling groups), taken together when it holds few observations --
+// or a single level M-2 group (large units are split for load balance; for
+// M = 2 the single level-0 group).  The observations of an item are
+// contiguous and all of them share the ancestors at levels 0..M-3: their
+// conditioning on those levels runs once per item (for a unit: products J
+// times wider, the ancestors' U read once).  The level M-2 step, the finest
+// children and the level M-2 posterior then run per group.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T> t, int keep) {
     LaSmem<T>& sm = la_smem<T>();
-    __shared__ long s_p;
+    __shared__ long s_u;
     const int r = t.r, L = t.L, m = t.M - 2;
     const long rr = (long)r * r, Lr = (long)L * r;
-    const long s2 = level_start(t.J, m), cnt2 = level_count(t.J, m);
+    const long s2 = level_start(t.J, m);
+    const long n_units = t.M >= 3 ? level_count(t.J, m - 1) : 0;
     T* ws = t.ws + blockIdx.x * t.ws_stride;
     double* wsd = t.wsd + blockIdx.x * t.wsd_stride;
     for (;;) {
         if (threadIdx.x == 0) {
             int q = atomicAdd(&t.queue[0], 1);
-            s_p = q < cnt2 ? t.par_order[q] : -1;
+            s_u = q < t.n_fin_items ? t.par_order[q] : -1;
         }
         __syncthreads();
-        const long ploc = s_p;
+        const long item = s_u;
         __syncthreads();
-        if (ploc < 0) break;
-        const long p = s2 + ploc;
-        const long clo = t.child_lo[ploc], chi = t.child_hi[ploc];
-        const long lo = t.obs_off[clo];
-        const int np = (int)(t.obs_off[chi] - lo);
+        if (item < 0) break;
+        // item < n_units: unit (level M-3 local index); else group item - n_units (level M-2 local index)
+        const bool unit = item < n_units;
+        const long g_lo = unit ? item * t.J : item - n_units, g_hi = unit ? g_lo + t.J : g_lo + 1;
+        const long ui = unit ? level_start(t.J, m - 1) + item : s2 + g_lo;  // region whose subtree is the item
         long anc[kMaxLevels];
-        anc[m] = p;
-        {
-            long c = p;
-            for (int a = m - 1; a >= 0; --a) {
+        if (m > 0) {
+            long c = unit ? ui : (ui - 1) / t.J;
+            anc[m - 1] = c;
+            for (int a = m - 2; a >= 0; --a) {
                 c = (c - 1) / t.J;
                 anc[a] = c;
             }
         }
-        double dterm = 0.0;
-        if (np > 0) {
-            T* Uf = t.Ufin + lo * Lr;  // (L r) x np, ld = L r
-            T* Bh = t.Bhat + lo * Lr;
-            // C(Q_{a_j}, S) for every ancestor at once, into the blocks of B^
+        const long ulo = t.sub_lo[ui];
+        const int nu = (int)(t.sub_hi[ui] - ulo);
+        if (m > 0 && nu > 0) {
+            // C(Q_{a_j}, S) of levels 0..M-3 for all observations of the unit, into B^
+            T* Uf = t.Ufin + ulo * Lr;  // (L r) x nu, ld = L r
+            T* Bh = t.Bhat + ulo * Lr;
             long aoff[kMaxLevels];
-            for (int j = 0; j < L; ++j) aoff[j] = anc[j] * r;
-            fill_cov_blocks<T>(g, t.pts, aoff, L, r, t.obs0 + lo, np, false, Bh, Lr, r, sm);
-            for (int j = 0; j < L; ++j) {
+            for (int j = 0; j < m; ++j) aoff[j] = anc[j] * r;
+            fill_cov_blocks<T>(g, t.pts, aoff, m, r, t.obs0 + ulo, nu, false, Bh, Lr, r, sm);
+            for (int j = 0; j < m; ++j) {
                 const long a = anc[j];
                 T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
                 if (j > 0) {
                     const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                    gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, Uf, Lr, (T)1, V, Lr, sm);
+                    gemm<T, true, false>(r, nu, j * r, (T)-1, Ua, (long)j * r, Uf, Lr, (T)1, V, Lr, sm);
                 }
-                gemm<T, false, false>(r, np, r, (T)1, t.Pinv + a * rr, r, V, Lr, (T)0, Uf + (long)j * r, Lr, sm);
-            }
-            int nmax = 0;
-            for (long c = clo; c < chi; ++c) nmax = max(nmax, (int)(t.obs_off[c + 1] - t.obs_off[c]));
-            const bool grouped = sizeof(T) == 8 && nmax <= kChildMax && np <= kGroupMax &&
-                                 chi - clo <= kThreads / 32;
-            if (grouped) dterm += finest_children_grouped<T>(g, t, clo, chi, lo, np, ws, sm);
-            for (long c = clo; c < chi && !grouped; ++c) {
-                const long o0 = t.obs_off[c];
-                const int n = (int)(t.obs_off[c + 1] - o0);
-                if (n == 0) continue;
-                T* S = t.Lsig + t.lsig_off[c];
-                fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n, sm);
-                __syncthreads();
-                gemm<T, true, false>(n, n, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, t.Ufin + o0 * Lr, Lr, (T)1, S, n,
-                                     sm);
-                double ld = 0.0;
-                const bool small = sizeof(T) == 8 && n <= 64;
-                T* Sinv = ws;  // n x n
-                int info = potrf_lower<T>(n, S, n, sm, &ld, small ? Sinv : nullptr, n);
-                double* ytc = t.yt + o0;
-                for (int e = threadIdx.x; e < n; e += kThreads) ytc[e] = t.y[o0 + e];
-                __syncthreads();
-                trsv_lower_f64<T>(n, S, n, ytc);
-                if (small) {
-                    // B^ = V L_Sigma^{-T}, in place: each 64-row tile of the product
-                    // reads exactly the rows it then writes
-                    gemm<T, false, true, true>((int)Lr, n, n, (T)1, t.Bhat + o0 * Lr, Lr, Sinv, n, (T)0,
-                                               t.Bhat + o0 * Lr, Lr, sm);
-                } else {
-                    trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
-                }
-                double part = 0.0;
-                for (int e = threadIdx.x; e < n; e += kThreads) part += ytc[e] * ytc[e];
-                double yy = cta_sum(part, sm);
-                if (threadIdx.x == 0) {
-                    dterm += yy + ld;
-                    if (info) report_error(t.err, t.n_int + c);
-                }
+                gemm<T, false, false>(r, nu, r, (T)1, t.Pinv + a * rr, r, V, Lr, (T)0, Uf + (long)j * r, Lr, sm);
             }
         }
-        if (threadIdx.x == 0) t.dfin[ploc] = dterm;
-        if (!t.fuse_post) continue;
-        dterm = 0.0;
-        // posterior of the parent at level m = M-2 from F = B^ rows, f = y~
-        const T* F = t.Bhat + lo * Lr;
-        const double* f = t.yt + lo;
-        if (t.factored[p]) {
-            T* Fo = m > 0 ? t.Fbuf[m & 1] + lo * (long)m * r : nullptr;
-            double* fo = m > 0 ? t.fbuf[m & 1] + lo : nullptr;
-            factored_step<T>(t, m, p, np, F, Lr, f, Fo, fo, keep != 0, ws, wsd, sm, dterm);
-        } else {
-            T* Aagg = ws;
-            double* wagg = wsd;
-            for (long e = threadIdx.x; e < n_slices(m + 1) * rr; e += kThreads) Aagg[e] = (T)0;
-            for (long e = threadIdx.x; e < Lr; e += kThreads) wagg[e] = 0.0;
+        for (long ploc = g_lo; ploc < g_hi; ++ploc) {
+            const long p = s2 + ploc;
+            const long clo = t.child_lo[ploc], chi = t.child_hi[ploc];
+            const long lo = t.obs_off[clo];
+            const int np = (int)(t.obs_off[chi] - lo);
+            double dterm = 0.0;
+            if (np > 0) {
+                // level M-2: the group's own parent p
+                T* Uf = t.Ufin + lo * Lr;
+                T* V = t.Bhat + lo * Lr + (long)m * r;
+                const long ap = p * r;
+                fill_cov_blocks<T>(g, t.pts, &ap, 1, r, t.obs0 + lo, np, false, V, Lr, 0, sm);
+                if (m > 0) {
+                    const T* Ua = t.U + t.u_off[m] + ploc * (long)m * rr;
+                    gemm<T, true, false>(r, np, m * r, (T)-1, Ua, (long)m * r, Uf, Lr, (T)1, V, Lr, sm);
+                }
+                gemm<T, false, false>(r, np, r, (T)1, t.Pinv + p * rr, r, V, Lr, (T)0, Uf + (long)m * r, Lr, sm);
+                int nmax = 0;
+                for (long c = clo; c < chi; ++c) nmax = max(nmax, (int)(t.obs_off[c + 1] - t.obs_off[c]));
+                const bool grouped = sizeof(T) == 8 && nmax <= kChildMax && np <= kGroupMax &&
+                                     chi - clo <= kThreads / 32;
+                if (grouped) dterm += finest_children_grouped<T>(g, t, clo, chi, lo, np, ws, sm);
+                for (long c = clo; c < chi && !grouped; ++c) {
+                    const long o0 = t.obs_off[c];
+                    const int n = (int)(t.obs_off[c + 1] - o0);
+                    if (n == 0) continue;
+                    T* S = t.Lsig + t.lsig_off[c];
+                    fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.obs0 + o0, n, true, S, n, sm);
+                    __syncthreads();
+                    gemm<T, true, false>(n, n, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, t.Ufin + o0 * Lr, Lr, (T)1, S,
+                                         n, sm);
+                    double ld = 0.0;
+                    const bool small = sizeof(T) == 8 && n <= 64;
+                    T* Sinv = ws;  // n x n
+                    int info = potrf_lower<T>(n, S, n, sm, &ld, small ? Sinv : nullptr, n);
+                    double* ytc = t.yt + o0;
+                    for (int e = threadIdx.x; e < n; e += kThreads) ytc[e] = t.y[o0 + e];
+                    __syncthreads();
+                    trsv_lower_f64<T>(n, S, n, ytc);
+                    if (small) {
+                        // B^ = V L_Sigma^{-T}, in place: each 64-row tile of the product
+                        // reads exactly the rows it then writes
+                        gemm<T, false, true, true>((int)Lr, n, n, (T)1, t.Bhat + o0 * Lr, Lr, Sinv, n, (T)0,
+                                                   t.Bhat + o0 * Lr, Lr, sm);
+                    } else {
+                        trsm_right_lower_trans<T>((int)Lr, n, S, n, t.Bhat + o0 * Lr, Lr, sm);
+                    }
+                    double part = 0.0;
+                    for (int e = threadIdx.x; e < n; e += kThreads) part += ytc[e] * ytc[e];
+                    double yy = cta_sum(part, sm);
+                    if (threadIdx.x == 0) {
+                        dterm += yy + ld;
+                        if (info) report_error(t.err, t.n_int + c);
+                    }
+                }
+            }
+            if (threadIdx.x == 0) t.dfin[ploc] = dterm;
+            if (!t.fuse_post) continue;
+            dterm = 0.0;
+            // posterior of the parent at level m = M-2 from F = B^ rows, f = y~
+            const T* F = t.Bhat + lo * Lr;
+            const double* f = t.yt + lo;
+            if (t.factored[p]) {
+                T* Fo = m > 0 ? t.Fbuf[m & 1] + lo * (long)m * r : nullptr;
+                double* fo = m > 0 ? t.fbuf[m & 1] + lo : nullptr;
+                factored_step<T>(t, m, p, np, F, Lr, f, Fo, fo, keep != 0, ws, wsd, sm, dterm);
+            } else {
+                T* Aagg = ws;
+                double* wagg = wsd;
+                for (long e = threadIdx.x; e < n_slices(m + 1) * rr; e += kThreads) Aagg[e] = (T)0;
+                for (long e = threadIdx.x; e < Lr; e += kThreads) wagg[e] = 0.0;
+                __syncthreads();
+                accumulate_factored<T>(t, m, np, F, Lr, f, Aagg, wagg, sm);
+                dense_step<T>(t, m, p, Aagg, wagg, keep != 0, Aagg + n_slices(m + 1) * rr, sm, dterm);
+            }
+            if (threadIdx.x == 0) t.dpost[p] = dterm;
             __syncthreads();
-            accumulate_factored<T>(t, m, np, F, Lr, f, Aagg, wagg, sm);
-            dense_step<T>(t, m, p, Aagg, wagg, keep != 0, Aagg + n_slices(m + 1) * rr, sm, dterm);
         }
-        if (threadIdx.x == 0) t.dpost[p] = dterm;
-        __syncthreads();
     }
 }
 
@@ -770,7 +801,7 @@ void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cud
 }
 template <typename T>
 void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
-    long cnt = level_count(t.J, t.M - 2);
+    long cnt = t.n_fin_items;
     k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, keep ? 1 : 0);
 }
 template <typename T>
