@@ -744,6 +744,33 @@ __device__ inline void trsv_lower_f64(int n, const T* L, long ldl, double* b) {
     __syncthreads();
 }
 
+// x = Linv b for a lower-triangular Linv (n x n, ld ldl) that is the inverse
+// of a factor: the triangular solve as a product, one row per thread.  x may
+// alias b.  Ends with a barrier.
+template <typename T>
+__device__ inline void trmv_lower_inv(int n, const T* Linv, long ldl, double* x, const double* b) {
+    double v[2] = {0.0, 0.0};
+    for (int h = 0; h < 2; ++h) {
+        const int q = threadIdx.x + h * kThreads;
+        if (q < n) {
+            double s0 = 0.0, s1 = 0.0;
+            int k = 0;
+            for (; k + 1 <= q; k += 2) {
+                s0 += (double)Linv[q + (long)k * ldl] * b[k];
+                s1 += (double)Linv[q + (long)(k + 1) * ldl] * b[k + 1];
+            }
+            if (k <= q) s0 += (double)Linv[q + (long)k * ldl] * b[k];
+            v[h] = s0 + s1;
+        }
+    }
+    __syncthreads();
+    for (int h = 0; h < 2; ++h) {
+        const int q = threadIdx.x + h * kThreads;
+        if (q < n) x[q] = v[h];
+    }
+    __syncthreads();
+}
+
 // Deterministic CTA sum (fixed thread -> element mapping and tree order).
 template <typename T>
 __device__ inline double cta_sum(double v, LaSmem<T>& sm) {

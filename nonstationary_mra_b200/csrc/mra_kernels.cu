@@ -166,7 +166,8 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
         part += f[q] * f[q];
     }
     double ff = cta_sum(part, sm);
-    trsv_lower_f64<T>(n, S, n, fp);
+    if (small) trmv_lower_inv<T>(n, Rinv, n, fp, fp);  // f' = R^{-1} f with the inverse formed above
+    else trsv_lower_f64<T>(n, S, n, fp);
     part = 0.0;
     for (int q = threadIdx.x; q < n; q += kThreads) part += fp[q] * fp[q];
     double pp = cta_sum(part, sm);
@@ -232,7 +233,8 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     double* v = t.vpost + i * r;
     for (int e = threadIdx.x; e < r; e += kThreads) v[e] = wagg[mr + e];
     __syncthreads();
-    trsv_lower_f64<T>(r, Lt, r, v);
+    if (small) trmv_lower_inv<T>(r, Ltinv, r, v, v);  // v = L~^{-1} w_m with the inverse formed above
+    else trsv_lower_f64<T>(r, Lt, r, v);
     double part = 0.0;
     for (int e = threadIdx.x; e < r; e += kThreads) part += v[e] * v[e];
     double vv = cta_sum(part, sm);
@@ -505,7 +507,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
                     double* ytc = t.yt + o0;
                     for (int e = threadIdx.x; e < n; e += kThreads) ytc[e] = t.y[o0 + e];
                     __syncthreads();
-                    trsv_lower_f64<T>(n, S, n, ytc);
+                    if (small) trmv_lower_inv<T>(n, Sinv, n, ytc, ytc);  // y~ = L_Sigma^{-1} y
+                    else trsv_lower_f64<T>(n, S, n, ytc);
                     if (small) {
                         // B^ = V L_Sigma^{-T}, in place: each 64-row tile of the product
                         // reads exactly the rows it then writes
