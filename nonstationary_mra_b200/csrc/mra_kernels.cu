@@ -140,6 +140,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
 // ---------------------------------------------------------------------------
 // posterior steps of one region (level m): factored and dense forms
 // ---------------------------------------------------------------------------
+// The products of the posterior steps go through a separate function: the
+// steps keep many values live across their products, and inlined there the
+// product loops would share (and spill) their registers.
+template <typename T, bool TA, bool TB>
+__device__ __noinline__ void gemm_call(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb,
+                                       T beta, T* C, long ldc, LaSmem<T>& sm) {
+    gemm<T, TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+}
+
 // Factored input (F: n rows of width (m+1) r, row stride ldF; f: n doubles).
 // Writes F' (n rows of width m r) to Fo and f' to fo when m > 0.
 template <typename T>
@@ -152,8 +161,8 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
     T* S = ws + (long)r * n;    // n x n
     T* Rinv = S + (long)n * n;  // n x n (n <= 64)
     // Y = L_i^{-1} F_m^T as a product with the stored inverse of the prior factor
-    gemm<T, false, false>(r, n, r, (T)1, t.Pinv + i * rr, r, F + mr, ldF, (T)0, Y, r, sm);
-    gemm<T, true, false>(n, n, r, (T)1, Y, r, Y, r, (T)0, S, n, sm);
+    gemm_call<T, false, false>(r, n, r, (T)1, t.Pinv + i * rr, r, F + mr, ldF, (T)0, Y, r, sm);
+    gemm_call<T, true, false>(n, n, r, (T)1, Y, r, Y, r, (T)0, S, n, sm);
     for (int q = threadIdx.x; q < n; q += kThreads) S[q + (long)q * n] += (T)1;
     __syncthreads();
     double ld = 0.0;
@@ -178,7 +187,7 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
     if (m > 0) {
         if (small) {
             // F' = F_{0..m-1} R^{-T}
-            gemm<T, false, true>((int)mr, n, n, (T)1, F, ldF, Rinv, n, (T)0, Fo, mr, sm);
+            gemm_call<T, false, true>((int)mr, n, n, (T)1, F, ldF, Rinv, n, (T)0, Fo, mr, sm);
         } else {
             for (long e = threadIdx.x; e < mr * n; e += kThreads) {
                 long x = e % mr, q = e / mr;
@@ -192,8 +201,8 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
         // predictive factors of the region: L~ L~^T = L L^T + F_m^T F_m, v = L~^{-1} F_m^T f,
         // G = L~^{-1} F_m^T F_{0..m-1}
         T* Lt = t.Lpost + i * rr;
-        gemm<T, false, true>(r, r, r, (T)1, Li, r, Li, r, (T)0, Lt, r, sm);
-        gemm<T, false, true>(r, r, n, (T)1, F + mr, ldF, F + mr, ldF, (T)1, Lt, r, sm);
+        gemm_call<T, false, true>(r, r, r, (T)1, Li, r, Li, r, (T)0, Lt, r, sm);
+        gemm_call<T, false, true>(r, r, n, (T)1, F + mr, ldF, F + mr, ldF, (T)1, Lt, r, sm);
         int info2 = potrf_lower<T>(r, Lt, r, sm, nullptr);
         double* v = t.vpost + i * r;
         for (int tt = threadIdx.x; tt < r; tt += kThreads) {
@@ -205,7 +214,7 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
         trsv_lower_f64<T>(r, Lt, r, v);
         if (m > 0) {
             T* Gi = t.G + t.u_off[m] + (i - level_start(t.J, m)) * mr * r;
-            gemm<T, false, true>(r, (int)mr, n, (T)1, F + mr, ldF, F, ldF, (T)0, Gi, r, sm);
+            gemm_call<T, false, true>(r, (int)mr, n, (T)1, F + mr, ldF, F, ldF, (T)0, Gi, r, sm);
             trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
         }
         if (info2 && threadIdx.x == 0) report_error(t.err, i);
@@ -222,7 +231,7 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     const long loc = i - level_start(t.J, m);
     const T* Lp = t.Lprior + i * rr;
     T* Lt = t.Lpost + i * rr;
-    gemm<T, false, true>(r, r, r, (T)1, Lp, r, Lp, r, (T)0, Lt, r, sm);
+    gemm_call<T, false, true>(r, r, r, (T)1, Lp, r, Lp, r, (T)0, Lt, r, sm);
     const T* Amm = Aagg + slice_index(m + 1, m, m) * rr;
     for (long e = threadIdx.x; e < rr; e += kThreads) Lt[e] += Amm[e];
     __syncthreads();
@@ -247,7 +256,7 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     if (small) {
         // G_j = L~^{-1} A_(j,m)^T
         for (int j = 0; j < m; ++j)
-            gemm<T, false, true>(r, r, r, (T)1, Ltinv, r, Aagg + slice_index(m + 1, j, m) * rr, r, (T)0,
+            gemm_call<T, false, true>(r, r, r, (T)1, Ltinv, r, Aagg + slice_index(m + 1, j, m) * rr, r, (T)0,
                                  Gi + (long)j * rr, r, sm);
     } else {
         for (long e = threadIdx.x; e < mr * r; e += kThreads) {
@@ -274,7 +283,7 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
         const long cnt = (long)(m - j) * rr;
         for (long e = threadIdx.x; e < cnt; e += kThreads) dst[e] = src[e];
         __syncthreads();
-        gemm<T, true, false>(r, (m - j) * r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)j * rr, r, (T)1, dst, r, sm);
+        gemm_call<T, true, false>(r, (m - j) * r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)j * rr, r, (T)1, dst, r, sm);
     }
 }
 
@@ -288,7 +297,7 @@ __device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
     if (n == 0) return;
     for (int j = 0; j <= m; ++j)
-        gemm<T, false, true>(r, (m + 1 - j) * r, n, (T)1, F + (long)j * r, ldF, F + (long)j * r, ldF, (T)1,
+        gemm_call<T, false, true>(r, (m + 1 - j) * r, n, (T)1, F + (long)j * r, ldF, F + (long)j * r, ldF, (T)1,
                              Aagg + slice_index(m + 1, j, j) * rr, r, sm);
     for (long x = threadIdx.x; x < mr1; x += kThreads) {
         double s = 0.0;
