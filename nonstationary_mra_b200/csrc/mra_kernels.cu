@@ -142,11 +142,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
 // ---------------------------------------------------------------------------
 // The products of the posterior steps go through a separate function: the
 // steps keep many values live across their products, and inlined there the
-// product loops would share (and spill) their registers.
-template <typename T, bool TA, bool TB>
+// product loops would share (and spill) their registers.  (The finest-level
+// kernel measured faster with its products inlined.)
+template <typename T, bool TA, bool TB, bool ONE_TILE = false>
 __device__ __noinline__ void gemm_call(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb,
                                        T beta, T* C, long ldc, LaSmem<T>& sm) {
-    gemm<T, TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+    gemm<T, TA, TB, ONE_TILE>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
 }
 
 // Factored input (F: n rows of width (m+1) r, row stride ldF; f: n doubles).
@@ -287,22 +288,30 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     }
 }
 
-// Aagg/wagg += the (A~, w~) of factored rows F (n x (m+1) r, row stride ldF), f.
+// Aagg/wagg += the (A~, w~) of factored rows F (n x (m+1) r, row stride ldF), f;
+// with `init` they are set instead (the first contribution: no zeroing pass).
 // The slices (j, j..m) of A~ are contiguous r x r blocks, so block row j is
 // one product F_j^T F_{j..m} (r x (m+1-j) r).
 template <typename T>
 __device__ __noinline__ void accumulate_factored(const DevTree<T>& t, int m, int n, const T* F, long ldF, const double* f, T* Aagg,
-                                    double* wagg, LaSmem<T>& sm) {
+                                    double* wagg, bool init, LaSmem<T>& sm) {
     const int r = t.r;
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
-    if (n == 0) return;
+    if (n == 0) {
+        if (init) {
+            for (long e = threadIdx.x; e < n_slices(m + 1) * rr; e += kThreads) Aagg[e] = (T)0;
+            for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = 0.0;
+            __syncthreads();
+        }
+        return;
+    }
     for (int j = 0; j <= m; ++j)
-        gemm_call<T, false, true>(r, (m + 1 - j) * r, n, (T)1, F + (long)j * r, ldF, F + (long)j * r, ldF, (T)1,
-                             Aagg + slice_index(m + 1, j, j) * rr, r, sm);
+        gemm_call<T, false, true>(r, (m + 1 - j) * r, n, (T)1, F + (long)j * r, ldF, F + (long)j * r, ldF,
+                                  init ? (T)0 : (T)1, Aagg + slice_index(m + 1, j, j) * rr, r, sm);
     for (long x = threadIdx.x; x < mr1; x += kThreads) {
         double s = 0.0;
         for (int q = 0; q < n; ++q) s += (double)F[(long)q * ldF + x] * f[q];
-        wagg[x] += s;
+        wagg[x] = init ? s : wagg[x] + s;
     }
     __syncthreads();
 }
@@ -548,10 +557,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
             } else {
                 T* Aagg = ws;
                 double* wagg = wsd;
-                for (long e = threadIdx.x; e < n_slices(m + 1) * rr; e += kThreads) Aagg[e] = (T)0;
-                for (long e = threadIdx.x; e < Lr; e += kThreads) wagg[e] = 0.0;
-                __syncthreads();
-                accumulate_factored<T>(t, m, np, F, Lr, f, Aagg, wagg, sm);
+                accumulate_factored<T>(t, m, np, F, Lr, f, Aagg, wagg, true, sm);
                 dense_step<T>(t, m, p, Aagg, wagg, keep != 0, Aagg + n_slices(m + 1) * rr, sm, dterm);
             }
             if (threadIdx.x == 0) t.dpost[p] = dterm;
@@ -593,10 +599,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
             } else {
                 T* Aagg = ws;
                 double* wagg = wsd;
-                for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = (T)0;
-                for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = 0.0;
-                __syncthreads();
-                accumulate_factored<T>(t, m, n, F, mr1, f, Aagg, wagg, sm);
+                accumulate_factored<T>(t, m, n, F, mr1, f, Aagg, wagg, true, sm);
                 dense_step<T>(t, m, i, Aagg, wagg, keep != 0, Aagg + ns_in * rr, sm, dterm);
             }
         } else if (t.factored[i]) {
@@ -608,9 +611,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
         } else {
             T* Aagg = ws;
             double* wagg = wsd;
-            for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = (T)0;
-            for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = 0.0;
-            __syncthreads();
+            bool first = true;  // the first contribution sets Aagg / wagg
             for (int cc = 1; cc <= t.J; ++cc) {
                 const long c = i * t.J + cc;
                 if (t.factored[c]) {
@@ -622,13 +623,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
                         ++cl;
                         hi = t.sub_hi[cl];
                     }
-                    accumulate_factored<T>(t, m, (int)(hi - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg, sm);
+                    accumulate_factored<T>(t, m, (int)(hi - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg, first, sm);
                 } else {
                     const long cl = c - s1;
-                    for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] += ain[cl * ns_in * rr + e];
-                    for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] += win[cl * mr1 + e];
+                    const T* as = ain + cl * ns_in * rr;
+                    const double* wsrc = win + cl * mr1;
+                    for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = first ? as[e] : Aagg[e] + as[e];
+                    for (long e = threadIdx.x; e < mr1; e += kThreads) wagg[e] = first ? wsrc[e] : wagg[e] + wsrc[e];
                     __syncthreads();
                 }
+                first = false;
             }
             dense_step<T>(t, m, i, Aagg, wagg, keep != 0, Aagg + ns_in * rr, sm, dterm);
         }
