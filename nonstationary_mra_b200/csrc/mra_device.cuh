@@ -429,7 +429,8 @@ __device__ __forceinline__ void warp_step_f64(AccD<NW>& acc, const double* sA, c
 // works on the current one.
 template <bool TA, bool TB, int NW>
 __device__ inline void gemm_f64(int M, int N, int K, double alpha, const double* A, long lda, const double* B,
-                                long ldb, double beta, double* C, long ldc, LaSmem<double>& sm) {
+                                long ldb, double beta, double* C, long ldc, LaSmem<double>& sm,
+                                const double* Cin = nullptr, long ldcin = 0) {
     constexpr int W = 16 * NW;                // CTA tile width
     constexpr int WM = 8 / NW;                // warps along M
     constexpr int PA = 64 * TK64 / kThreads;  // A elements per thread per slab (8)
@@ -494,7 +495,8 @@ __device__ inline void gemm_f64(int M, int N, int K, double alpha, const double*
                         for (int h = 0; h < 2; ++h) {
                             if (r < M && c + h < N) {
                                 double* p = C + r + (long)(c + h) * ldc;
-                                *p = beta == 0.0 ? alpha * acc.v[i][j][h] : alpha * acc.v[i][j][h] + beta * *p;
+                                const double* q = Cin ? Cin + r + (long)(c + h) * ldcin : p;
+                                *p = beta == 0.0 ? alpha * acc.v[i][j][h] : alpha * acc.v[i][j][h] + beta * *q;
                             }
                         }
                     }
@@ -547,7 +549,8 @@ __device__ __forceinline__ void warp_step_tf32x3(AccF& acc, const LaSmem<float>&
 
 template <bool TA, bool TB>
 __device__ inline void gemm_f32(int M, int N, int K, float alpha, const float* A, long lda, const float* B, long ldb,
-                                float beta, float* C, long ldc, LaSmem<float>& sm) {
+                                float beta, float* C, long ldc, LaSmem<float>& sm, const float* Cin = nullptr,
+                                long ldcin = 0) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
     constexpr int PER = TK * TM / kThreads;  // elements of each operand per thread per slab (4)
@@ -613,7 +616,8 @@ __device__ inline void gemm_f32(int M, int N, int K, float alpha, const float* A
                         const int rr = r + (q >> 1) * 8, cc = c + (q & 1);
                         if (rr < M && cc < N) {
                             float* p = C + rr + (long)cc * ldc;
-                            *p = beta == 0.f ? alpha * acc.v[i][j][q] : alpha * acc.v[i][j][q] + beta * *p;
+                            const float* qi = Cin ? Cin + rr + (long)cc * ldcin : p;
+                            *p = beta == 0.f ? alpha * acc.v[i][j][q] : alpha * acc.v[i][j][q] + beta * *qi;
                         }
                     }
                 }
@@ -622,7 +626,8 @@ __device__ inline void gemm_f32(int M, int N, int K, float alpha, const float* A
     __syncthreads();
 }
 
-// C = alpha * op(A) * op(B) + beta * C; op(A): M x K, op(B): K x N, column-major,
+// C = alpha * op(A) * op(B) + beta * Cin (Cin = C unless given, ld ldcin);
+// op(A): M x K, op(B): K x N, column-major,
 // any leading dimensions; A and B in global memory.  beta == 0 never reads C.
 // Ends with a barrier.
 // FP64 tile width (NW) per product-width bucket (N <= 16, N <= 32, wider),
@@ -638,14 +643,14 @@ __constant__ int c_gemm_nw[3] = {1, 2, 4};
 // would read columns the first one has already overwritten.
 template <typename T, bool TA, bool TB, bool ONE_TILE = false>
 __device__ inline void gemm(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta, T* C,
-                            long ldc, LaSmem<T>& sm) {
+                            long ldc, LaSmem<T>& sm, const T* Cin = nullptr, long ldcin = 0) {
     if constexpr (sizeof(T) == 8) {
         const int nw = ONE_TILE ? (N <= 16 ? 1 : (N <= 32 ? 2 : 4)) : c_gemm_nw[N <= 16 ? 0 : (N <= 32 ? 1 : 2)];
-        if (nw == 1) gemm_f64<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
-        else if (nw == 2) gemm_f64<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
-        else gemm_f64<TA, TB, 4>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        if (nw == 1) gemm_f64<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
+        else if (nw == 2) gemm_f64<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
+        else gemm_f64<TA, TB, 4>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
     } else {
-        gemm_f32<TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+        gemm_f32<TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
     }
 }
 

@@ -146,8 +146,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
 // kernel measured faster with its products inlined.)
 template <typename T, bool TA, bool TB, bool ONE_TILE = false>
 __device__ __noinline__ void gemm_call(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb,
-                                       T beta, T* C, long ldc, LaSmem<T>& sm) {
-    gemm<T, TA, TB, ONE_TILE>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm);
+                                       T beta, T* C, long ldc, LaSmem<T>& sm, const T* Cin = nullptr,
+                                       long ldcin = 0) {
+    gemm<T, TA, TB, ONE_TILE>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
 }
 
 // Factored input (F: n rows of width (m+1) r, row stride ldF; f: n doubles).
@@ -276,15 +277,13 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
         wo[x] = wagg[x] - s;
     }
     // A_out(j, j..m-1) = A(j, j..m-1) - G_j^T G_{j..m-1}: both slice rows are
-    // contiguous r x r blocks, one copy and one product per j
+    // contiguous r x r blocks, one product per j reading A from Aagg
     T* ao = t.aout[m & 1] + loc * n_slices(m) * rr;
     for (int j = 0; j < m; ++j) {
         T* dst = ao + slice_index(m, j, j) * rr;
         const T* src = Aagg + slice_index(m + 1, j, j) * rr;
-        const long cnt = (long)(m - j) * rr;
-        for (long e = threadIdx.x; e < cnt; e += kThreads) dst[e] = src[e];
-        __syncthreads();
-        gemm_call<T, true, false>(r, (m - j) * r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)j * rr, r, (T)1, dst, r, sm);
+        gemm_call<T, true, false>(r, (m - j) * r, r, (T)-1, Gi + (long)j * rr, r, Gi + (long)j * rr, r, (T)1, dst, r,
+                                  sm, src, r);
     }
 }
 
