@@ -257,30 +257,34 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 // ... < q_end (straight-line distance, nonstationary): writes ob[(qoff + q) ld].
 // NU: 1 exponential, 3 Matern 3/2; PREF: 0 prefactor x^1.5, 1 prefactor x.
 // Entry: sqrt(s1 s2) pre(x) matern(h), x = 2 b1 b2 / (b1^2 + b2^2),
-// h = scale sqrt(2 d^2 / (b1^2 + b2^2)).  Every parameter is in registers so
-// the loop carries no reloads; one reciprocal, one inverse square root and
-// one exponential per entry, none with a branch.
+// h = scale sqrt(2 d^2 / (b1^2 + b2^2)).  With g = b^2 / (2 scale^2) staged per
+// point, w = 1 / (g1 + g2) gives h = sqrt(d^2 w) and x = b1 b2 w / scale^2,
+// so the entry is (sqrt(s1) b1 / scale^2) (sqrt(s2) b2) w matern(h) for
+// PREF 1.  Every parameter is in registers so the loop carries no reloads;
+// one reciprocal, one inverse square root and one exponential per entry,
+// none with a branch.
 template <typename T, int NU, int PREF>
 __device__ __noinline__ void fill_row_fast(const double* __restrict__ sx, const double* __restrict__ sy,
                                            const double* __restrict__ sz, const double* __restrict__ ss,
-                                           const double* __restrict__ sb, const double* __restrict__ sb2, double pc0,
-                                           double pc1, double pc2, double ssa, double ba, double hs, int q_begin,
-                                           int q_end, int q_step, int qoff, T* __restrict__ ob, long ld) {
-    const double ba2 = ba * ba, c2 = 2.0 * ba * ssa;
+                                           const double* __restrict__ sb, const double* __restrict__ sg,
+                                           const double* __restrict__ ssb, double pc0, double pc1, double pc2,
+                                           double ssa, double ba, double ga, double ihs2, int q_begin, int q_end,
+                                           int q_step, int qoff, T* __restrict__ ob, long ld) {
+    const double ca = ssa * ba * ihs2, ba_h = ba * ihs2;
 #pragma unroll 4
     for (int q = q_begin; q < q_end; q += q_step) {
         const double dx = sx[q] - pc0, dy = sy[q] - pc1, dz = sz[q] - pc2;
         const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
-        const double ibms = rcp_nr(ba2 + sb2[q]);  // 1 / (b1^2 + b2^2)
-        const double u = 2.0 * d2 * ibms;
-        const double h = u > 1e-300 ? hs * (u * rsqrt_nr(u)) : 0.0;
+        const double w = rcp_nr(ga + sg[q]);  // 2 scale^2 / (b1^2 + b2^2)
+        const double u = d2 * w;              // h^2
+        const double h = u > 1e-300 ? u * rsqrt_nr(u) : 0.0;
         const double em = exp_neg(h);
         const double m = NU == 3 ? (1.0 + h) * em : em;
         double v;
         if (PREF == 1) {
-            v = (c2 * ss[q]) * (sb[q] * ibms) * m;
+            v = (ca * ssb[q]) * w * m;
         } else {
-            const double x = 2.0 * ba * sb[q] * ibms;
+            const double x = ba_h * sb[q] * w;
             v = (ssa * ss[q]) * (x * sqrt(x)) * m;
         }
         ob[(long)(qoff + q) * ld] = (T)v;
@@ -289,7 +293,7 @@ __device__ __noinline__ void fill_row_fast(const double* __restrict__ sx, const 
 
 // out[t + q*ld] = C(A_{a0+t}, B_{b0+q}), t < na, q < nb.  When `self` the
 // diagonal (t == q) is sigma^2 + tau^2 (evaluate_covariance.cpp:103,307).
-// The column points (coordinates, sqrt(sigma^2), beta, beta^2) are staged in
+// The column points (coordinates, sqrt(sigma^2), beta and two products) are staged in
 // shared memory in chunks, each thread keeps one row point in registers and
 // walks columns strided by the number of row groups (consecutive threads
 // write consecutive rows).  The straight-line nonstationary FP64 case with
@@ -308,7 +312,8 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
     double* sz = sy + CH;
     double* ss = sz + CH;
     double* sb = ss + CH;
-    double* sb2 = sb + CH;  // FP64 fast path only (6 CH doubles fit the FP64 tile buffers)
+    double* sg = sb + CH;   // FP64 fast path only: beta^2 / (2 scale^2) and sqrt(sigma^2) beta
+    double* ssb = sg + CH;  // (7 CH doubles fit the FP64 tile buffers)
     const int tid = threadIdx.x, nt = blockDim.x;
     const int R = nblk * na;  // all rows of all blocks
     const int rows = R < nt ? R : nt;
@@ -318,6 +323,7 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
     const int nu = g.nu_x2, pk = g.pref_kind;
     const bool fast = sizeof(T) == 8 && g.nonstat && g.distance != 1 && pk != 2;
     const double hs = g.dist_scale * (nu == 3 ? 1.7320508075688772 : 1.0);
+    const double ihs2 = 1.0 / (hs * hs), ih2 = 0.5 * ihs2;
     for (int q0 = 0; q0 < nb; q0 += CH) {
         const int qn = nb - q0 < CH ? nb - q0 : CH;
         __syncthreads();
@@ -329,7 +335,10 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
             ss[e] = fast ? sqrt(P.s2[ib]) : P.s2[ib];
             const double bb = P.beta[ib];
             sb[e] = bb;
-            if (fast) sb2[e] = bb * bb;
+            if (fast) {
+                sg[e] = bb * bb * ih2;
+                ssb[e] = ss[e] * bb;
+            }
         }
         __syncthreads();
         if (!worker) continue;
@@ -340,15 +349,19 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
                 T* ob = out + kb * blk + t;
                 const double pc0 = P.c0[ia], pc1 = P.c1[ia], pc2 = P.c2[ia];
                 const double sa = P.s2[ia], ba = P.beta[ia];
-                const double ssa = sqrt(sa);
+                const double ssa = sqrt(sa), ga = ba * ba * ih2;
                 if (nu == 3 && pk == 1)
-                    fill_row_fast<T, 3, 1>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                    fill_row_fast<T, 3, 1>(sx, sy, sz, ss, sb, sg, ssb, pc0, pc1, pc2, ssa, ba, ga, ihs2, tq, qn, cols,
+                                           q0, ob, ld);
                 else if (nu == 3)
-                    fill_row_fast<T, 3, 0>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                    fill_row_fast<T, 3, 0>(sx, sy, sz, ss, sb, sg, ssb, pc0, pc1, pc2, ssa, ba, ga, ihs2, tq, qn, cols,
+                                           q0, ob, ld);
                 else if (pk == 1)
-                    fill_row_fast<T, 1, 1>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                    fill_row_fast<T, 1, 1>(sx, sy, sz, ss, sb, sg, ssb, pc0, pc1, pc2, ssa, ba, ga, ihs2, tq, qn, cols,
+                                           q0, ob, ld);
                 else
-                    fill_row_fast<T, 1, 0>(sx, sy, sz, ss, sb, sb2, pc0, pc1, pc2, ssa, ba, hs, tq, qn, cols, q0, ob, ld);
+                    fill_row_fast<T, 1, 0>(sx, sy, sz, ss, sb, sg, ssb, pc0, pc1, pc2, ssa, ba, ga, ihs2, tq, qn, cols,
+                                           q0, ob, ld);
                 // the diagonal of a self block, whose entry this thread has just written
                 if (self && kb == 0) {
                     const int qd = t - q0;
