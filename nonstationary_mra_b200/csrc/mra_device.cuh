@@ -763,22 +763,24 @@ __device__ inline void trsv_lower_f64(int n, const T* L, long ldl, double* b) {
 }
 
 // x = Linv b for a lower-triangular Linv (n x n, ld ldl) that is the inverse
-// of a factor: the triangular solve as a product, one row per thread.  x may
-// alias b.  Ends with a barrier.
+// of a factor, stored with exact zeros above its diagonal: the triangular
+// solve as a product, one row per thread, every row over all n columns (a
+// uniform trip count, unrolled, so the loads of a row are in flight
+// together).  x may alias b.  Ends with a barrier.
 template <typename T>
 __device__ inline void trmv_lower_inv(int n, const T* Linv, long ldl, double* x, const double* b) {
     double v[2] = {0.0, 0.0};
     for (int h = 0; h < 2; ++h) {
         const int q = threadIdx.x + h * kThreads;
         if (q < n) {
-            double s0 = 0.0, s1 = 0.0;
+            double s[4] = {0.0, 0.0, 0.0, 0.0};
             int k = 0;
-            for (; k + 1 <= q; k += 2) {
-                s0 += (double)Linv[q + (long)k * ldl] * b[k];
-                s1 += (double)Linv[q + (long)(k + 1) * ldl] * b[k + 1];
+            for (; k + 8 <= n; k += 8) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) s[u & 3] += (double)Linv[q + (long)(k + u) * ldl] * b[k + u];
             }
-            if (k <= q) s0 += (double)Linv[q + (long)k * ldl] * b[k];
-            v[h] = s0 + s1;
+            for (; k < n; ++k) s[0] += (double)Linv[q + (long)k * ldl] * b[k];
+            v[h] = (s[0] + s[1]) + (s[2] + s[3]);
         }
     }
     __syncthreads();
