@@ -73,6 +73,9 @@ def parse_args():
     p.add_argument("--sweep", action="store_true",
                    help="instead of the log-likelihood line: the scaling sweep n in {1M, 2M, 4M} x M in "
                         "{10, 11, 12} x r in {32, 64, 128} (one JSON line per case)")
+    p.add_argument("--predict", action="store_true",
+                   help="instead of the log-likelihood line: prediction throughput on the workload with its "
+                        "prediction points (log-likelihood with the predictive factors kept, then prediction)")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -382,10 +385,54 @@ def sweep_arm(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def predict_arm(args):
+    """Prediction throughput: the workload's prediction points resident with the
+    tree; one step = log-likelihood with the predictive factors kept + the
+    prediction of every point (the reference's likelihood() + predict()).
+    Reports predictions/s of the whole step and of the prediction launch
+    alone (CUDA events on the library's stream)."""
+    from nonstationary_mra_b200 import api, capi, synth
+    cfg = synth.CONFIGS[args.config]
+    line = {"metric": "MRA predictions/sec (likelihood + predict)", "unit": "predictions/s",
+            "workload": workload_name(cfg), "n_pred": cfg.n_pred}
+    try:
+        xy, pred, theta, md, st = make_problem(cfg, with_pred=True)
+        ctx = api.Context(st, md)
+    except capi.MRAError as exc:
+        line.update(value=None, infeasible=str(exc)[:200])
+        print(json.dumps(line), flush=True)
+        return
+    try:
+        y = draw_values(ctx, st, cfg.seed + 7)
+        ctx.set_obs_values(y)
+        ctx.set_theta()
+        for _ in range(max(args.warmup, 1)):
+            ctx.predict()
+        steps = max(args.steps, 1)
+        ctx.timer_start()
+        for _ in range(steps):
+            mean, var = ctx.predict()
+        ms = ctx.timer_stop() / steps
+        stats = ctx.stats()
+        ms_kernel = sum(l["ms"] for l in stats["launches"] if l["kernel"] == "predict")
+        line.update(value=st.n_pred / (ms * 1e-3), ms_per_step=ms, predict_launch_ms=ms_kernel,
+                    predict_launch_per_s=st.n_pred / (ms_kernel * 1e-3) if ms_kernel > 0 else None,
+                    device_gb=stats["bytes_device"] / 1e9, mean_abs=float(np.mean(np.abs(mean))),
+                    steps=steps, warmup=args.warmup)
+    except capi.MRAError as exc:
+        line.update(value=None, failed=str(exc)[:200])
+    finally:
+        ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.fit:
         fit_arm(args)
+        return
+    if args.predict:
+        predict_arm(args)
         return
     if args.sweep:
         sweep_arm(args)

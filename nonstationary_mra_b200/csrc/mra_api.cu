@@ -408,6 +408,9 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     TALLOC(t.Lsig, T, prior_part ? h.lsig_off[c->n_fin] : 1);
     TALLOC(t.Lpost, T, need_lpost_g ? c->n_int * rr : 1);
     TALLOC(t.G, T, need_lpost_g && c->have_pred ? u_total : 1);
+    // inverses of the posterior factors, so that prediction multiplies instead of solving
+    t.Lpinv = nullptr;
+    if (sizeof(T) == 8 && post_part && c->have_pred && r <= 64) TALLOC(t.Lpinv, T, c->n_int * rr);
     for (int p = 0; p < 2; ++p) {
         TALLOC(t.aout[p], T, aout_sz[p]);
         TALLOC(t.wout[p], double, wout_sz[p]);

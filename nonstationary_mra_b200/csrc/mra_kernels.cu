@@ -205,7 +205,8 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
         T* Lt = t.Lpost + i * rr;
         gemm_call<T, false, true>(r, r, r, (T)1, Li, r, Li, r, (T)0, Lt, r, sm);
         gemm_call<T, false, true>(r, r, n, (T)1, F + mr, ldF, F + mr, ldF, (T)1, Lt, r, sm);
-        int info2 = potrf_lower<T>(r, Lt, r, sm, nullptr);
+        T* Lti = t.Lpinv ? t.Lpinv + i * rr : nullptr;  // L~^{-1}, kept for prediction
+        int info2 = potrf_lower<T>(r, Lt, r, sm, nullptr, Lti, r);
         double* v = t.vpost + i * r;
         for (int tt = threadIdx.x; tt < r; tt += kThreads) {
             double s = 0.0;
@@ -213,11 +214,15 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
             v[tt] = s;
         }
         __syncthreads();
-        trsv_lower_f64<T>(r, Lt, r, v);
+        if (Lti) trmv_lower_inv<T>(r, Lti, r, v, v);
+        else trsv_lower_f64<T>(r, Lt, r, v);
         if (m > 0) {
             T* Gi = t.G + t.u_off[m] + (i - level_start(t.J, m)) * mr * r;
             gemm_call<T, false, true>(r, (int)mr, n, (T)1, F + mr, ldF, F, ldF, (T)0, Gi, r, sm);
-            trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
+            // G = L~^{-1} G in place: one row tile (r <= 64) reads all of its
+            // column block before writing it
+            if (Lti) gemm_call<T, false, false>(r, (int)mr, r, (T)1, Lti, r, Gi, r, (T)0, Gi, r, sm);
+            else trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
         }
         if (info2 && threadIdx.x == 0) report_error(t.err, i);
     }
@@ -238,8 +243,10 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     for (long e = threadIdx.x; e < rr; e += kThreads) Lt[e] += Amm[e];
     __syncthreads();
     double ld = 0.0;
-    T* Ltinv = Gw + mr * r;  // r x r scratch after the G scratch
-    const bool small = sizeof(T) == 8 && r <= 64 && m > 0;
+    // L~^{-1}: kept for prediction when that is on, else an r x r scratch after the G scratch
+    const bool kept = keep && t.Lpinv;
+    T* Ltinv = kept ? t.Lpinv + i * rr : Gw + mr * r;
+    const bool small = sizeof(T) == 8 && r <= 64 && (m > 0 || kept);
     int info = potrf_lower<T>(r, Lt, r, sm, &ld, small ? Ltinv : nullptr, r);
     double* v = t.vpost + i * r;
     for (int e = threadIdx.x; e < r; e += kThreads) v[e] = wagg[mr + e];
@@ -675,13 +682,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(r, np, j * r, (T)-1, Ua, (long)j * r, P, Lr, (T)1, Cj, Lr, sm);
             }
-            for (long e = threadIdx.x; e < (long)r * np; e += kThreads) {
-                int tt = (int)(e % r);
-                long q = e / r;
-                P[(long)j * r + tt + q * Lr] = Cj[tt + q * Lr];
-            }
-            __syncthreads();
-            trsm_left_lower<T>(r, np, t.Lprior + a * rr, r, P + (long)j * r, Lr, sm);
+            // P_j = L_a^{-1} C_j as a product with the stored inverse of the prior factor
+            gemm<T, false, false>(r, np, r, (T)1, t.Pinv + a * rr, r, Cj, Lr, (T)0, P + (long)j * r, Lr, sm);
         }
         double* mean = t.mean + p0;
         double* var = t.var + p0;
@@ -718,7 +720,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
         for (int j = L - 1; j >= 0; --j) {
             const long a = anc[j];
             T* KcB = Bt + (long)j * r;
-            trsm_left_lower<T>(r, np, t.Lpost + a * rr, r, KcB, Lr, sm);
+            if (t.Lpinv) {
+                // L~_a^{-1} KcB in place (one row tile, r <= 64)
+                gemm<T, false, false>(r, np, r, (T)1, t.Lpinv + a * rr, r, KcB, Lr, (T)0, KcB, Lr, sm);
+            } else {
+                trsm_left_lower<T>(r, np, t.Lpost + a * rr, r, KcB, Lr, sm);
+            }
             if (j > 0) {
                 const T* Ga = t.G + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(j * r, np, r, (T)-1, Ga, r, KcB, Lr, (T)1, Bt, Lr, sm);

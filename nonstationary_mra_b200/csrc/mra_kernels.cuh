@@ -47,6 +47,7 @@ struct DevTree {
     T* Lpost;                  // [n_int][r*r]
     double* vpost;             // [n_int][r]
     T* G;                      // like U: [J^m][r x (m r)], ld = r (prediction mode)
+    T* Lpinv;                  // [n_int][r*r] inverse of each posterior factor (FP64 prediction mode, r <= 64), else null
     double* dpost;             // [n_int] posterior log-lik terms
     double* dfin;              // [J^(M-2)] finest-level log-lik terms of each sibling group
     int fuse_post;             // 1: the finest-group kernel also runs the level M-2 posterior
