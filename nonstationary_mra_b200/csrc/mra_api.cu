@@ -141,7 +141,7 @@ mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 
 // Host-side description of the tree used for sizing, scheduling and FLOP counts.
 struct HostTree {
-    std::vector<int64_t> nfin, npred, obs_off, pred_off, fin_anc, fin_order, lsig_off, pc_off;
+    std::vector<int64_t> nfin, npred, obs_off, pred_off, fin_anc, pred_order, lsig_off, pc_off;
     std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi;
     std::vector<int8_t> factored;
 };
@@ -365,7 +365,7 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     t.pred0 = c->n_int * r + c->n_obs;
     t.pts = pts;
     t.y = y;
-    t.obs_off = idx[0]; t.pred_off = idx[1]; t.fin_anc = idx[2]; t.fin_order = idx[3]; t.lsig_off = idx[4];
+    t.obs_off = idx[0]; t.pred_off = idx[1]; t.fin_anc = idx[2]; t.pred_order = idx[3]; t.lsig_off = idx[4];
     t.pc_off = idx[5]; t.child_lo = idx[6]; t.child_hi = idx[7]; t.par_order = idx[8]; t.sub_lo = idx[9];
     t.sub_hi = idx[10];
     t.n_fin_items = (long)h.par_order.size();
@@ -549,7 +549,6 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     h.fin_anc.assign(n_fin * L, 0);
     h.lsig_off.assign(n_fin + 1, 0);
     h.pc_off.assign(n_fin + 1, 0);
-    h.fin_order.assign(n_fin, 0);
     for (long k = 0; k <= n_fin; ++k) {
         h.obs_off[k] = (int64_t)s->obs_offset[k];
         if (have_pred_arr) h.pred_off[k] = (int64_t)s->pred_offset[k];
@@ -563,11 +562,20 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         }
         h.lsig_off[k + 1] = h.lsig_off[k] + h.nfin[k] * h.nfin[k];
         h.pc_off[k + 1] = h.pc_off[k] + h.nfin[k] * h.npred[k];
-        h.fin_order[k] = k;
     }
-    std::stable_sort(h.fin_order.begin(), h.fin_order.end(), [&](int64_t a, int64_t b) {
-        return h.npred[a] * (h.nfin[a] + 1) > h.npred[b] * (h.nfin[b] + 1);
-    });
+    // prediction work items: level M-2 regions (their finest children together),
+    // most expensive first
+    {
+        std::vector<double> cost(cnt2, 0.0);
+        for (long k = 0; k < n_fin; ++k) {
+            const long q = (long)s->finest_parent[k] - lvl2;
+            cost[q] += (double)h.npred[k] * (double)(64L * L + h.nfin[k] + 1);
+        }
+        h.pred_order.resize(cnt2);
+        for (long q = 0; q < cnt2; ++q) h.pred_order[q] = q;
+        std::stable_sort(h.pred_order.begin(), h.pred_order.end(),
+                         [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    }
     // subtree observation ranges and the factored / dense decision per interior region
     h.sub_lo.assign(n_int, 0);
     h.sub_hi.assign(n_int, 0);
@@ -642,7 +650,7 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     }
     double* y = c->alloc<double>(n_obs, &ce);
     if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: y"));
-    const std::vector<int64_t>* tabs[11] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.fin_order, &h.lsig_off,
+    const std::vector<int64_t>* tabs[11] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.pred_order, &h.lsig_off,
                                             &h.pc_off, &h.child_lo, &h.child_hi, &h.par_order, &h.sub_lo, &h.sub_hi};
     int64_t* idx[11];
     for (int q = 0; q < 11; ++q) {

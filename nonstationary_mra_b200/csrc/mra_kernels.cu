@@ -18,7 +18,8 @@
 //   k_posterior_level(m) levels M-3..0 (...-posterior-inference.cpp:14-265,
 //                       class_approximation.cpp:186-306)
 //   k_reduce            deterministic sum of the per-region terms
-//   k_predict           prediction, one CTA per finest region with predictions
+//   k_predict           prediction, one CTA per level M-2 region (its finest
+//                       children's predictions together)
 //                       (...-prior.cpp:271-392, class_approximation-predict.cpp:105-189)
 //
 // Posterior representation.  A region's contribution to its parent is the pair
@@ -650,27 +651,61 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
 // ---------------------------------------------------------------------------
 // a12: prediction
 // ---------------------------------------------------------------------------
+// For every prediction q < np, one warp forms ss = sum_x c_x^2 and
+// mm = sum_x c_x v_x over the column c = C + q ldc (len entries; v may be
+// null) with a fixed lane -> entry mapping and shuffle tree, and lane 0 applies
+// var[q] += sgn * ss, mean[q] = (add_mean ? mean[q] : 0) + mm.  Ends with a barrier.
+template <typename T>
+__device__ inline void predict_column_sums(int np, const T* C, long ldc, int len, const double* v, double sgn,
+                                           bool add_mean, double* var, double* mean) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = w; q < np; q += kThreads / 32) {
+        const T* col = C + (long)q * ldc;
+        double ss = 0.0, mm = 0.0;
+        for (int x = lane; x < len; x += 32) {
+            const double c = (double)col[x];
+            ss += c * c;
+            if (v) mm += c * v[x];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            mm += __shfl_xor_sync(0xffffffffu, mm, o);
+        }
+        if (lane == 0) {
+            var[q] += sgn * ss;
+            if (v) mean[q] = (add_mean ? mean[q] : 0.0) + mm;
+        }
+    }
+    __syncthreads();
+}
+
+// One CTA per level M-2 region: the finest children of a region share all of
+// their ancestors, so the conditioning of the group's predictions on the
+// ancestors (prior part) and the posterior pass back over the ancestors run
+// once for all of them; only the part of each finest region's own
+// observations runs per child.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
     LaSmem<T>& sm = la_smem<T>();
     __shared__ long s_k;
     const int r = t.r, L = t.L;
     const long rr = (long)r * r, Lr = (long)L * r;
+    const long cnt2 = level_count(t.J, t.M - 2);
     for (;;) {
         if (threadIdx.x == 0) {
             int q = atomicAdd(&t.queue[1], 1);
-            s_k = q < t.n_fin ? t.fin_order[q] : -1;
+            s_k = q < cnt2 ? t.pred_order[q] : -1;
         }
         __syncthreads();
-        const long k = s_k;
+        const long gl = s_k;
         __syncthreads();
-        if (k < 0) break;
-        const long p0 = t.pred_off[k];
-        const int np = (int)(t.pred_off[k + 1] - p0);
+        if (gl < 0) break;
+        const long clo = t.child_lo[gl], chi = t.child_hi[gl];
+        if (chi <= clo) continue;
+        const long p0 = t.pred_off[clo];
+        const int np = (int)(t.pred_off[chi] - p0);
         if (np == 0) continue;
-        const long o0 = t.obs_off[k];
-        const int n = (int)(t.obs_off[k + 1] - o0);
-        const int64_t* anc = t.fin_anc + k * L;
+        const int64_t* anc = t.fin_anc + clo * L;  // shared by every finest child of the region
         T* P = t.P + p0 * Lr;
         T* Bt = t.Bt + p0 * Lr;
         for (int j = 0; j < L; ++j) {
@@ -688,34 +723,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
         double* mean = t.mean + p0;
         double* var = t.var + p0;
         for (int q = threadIdx.x; q < np; q += kThreads) {
-            long ip = t.pred0 + p0 + q;
-            double s = t.pts.s2[ip] + t.pts.t2[ip];
-            const T* col = P + (long)q * Lr;
-            double ss = 0.0;
-            for (long x = 0; x < Lr; ++x) ss += (double)col[x] * (double)col[x];
-            var[q] = s - ss;
+            const long ip = t.pred0 + p0 + q;
+            var[q] = t.pts.s2[ip] + t.pts.t2[ip];
             mean[q] = 0.0;
         }
         __syncthreads();
-        if (n > 0) {
-            T* Pc = t.Pc + t.pc_off[k];  // n x np, ld = n
-            fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.pred0 + p0, np, false, Pc, n, sm);
+        predict_column_sums<T>(np, P, Lr, (int)Lr, nullptr, -1.0, false, var, mean);
+        for (long k = clo; k < chi; ++k) {
+            const long pk = t.pred_off[k];
+            const int npk = (int)(t.pred_off[k + 1] - pk);
+            const long o0 = t.obs_off[k];
+            const int n = (int)(t.obs_off[k + 1] - o0);
+            if (npk == 0 || n == 0) continue;
+            T* Pk = t.P + pk * Lr;
+            T* Pc = t.Pc + t.pc_off[k];  // n x npk, ld = n
+            fill_cov<T>(g, t.pts, t.obs0 + o0, n, t.pred0 + pk, npk, false, Pc, n, sm);
             __syncthreads();
-            gemm<T, true, false>(n, np, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, P, Lr, (T)1, Pc, n, sm);
-            trsm_left_lower<T>(n, np, t.Lsig + t.lsig_off[k], n, Pc, n, sm);
-            const double* yt = t.yt + o0;
-            for (int q = threadIdx.x; q < np; q += kThreads) {
-                const T* col = Pc + (long)q * n;
-                double ss = 0.0, mm = 0.0;
-                for (int x = 0; x < n; ++x) {
-                    ss += (double)col[x] * (double)col[x];
-                    mm += (double)col[x] * yt[x];
-                }
-                var[q] -= ss;
-                mean[q] = mm;
-            }
-            __syncthreads();
-            gemm<T, false, false>((int)Lr, np, n, (T)-1, t.Bhat + o0 * Lr, Lr, Pc, n, (T)1, Bt, Lr, sm);
+            gemm<T, true, false>(n, npk, (int)Lr, (T)-1, t.Ufin + o0 * Lr, Lr, Pk, Lr, (T)1, Pc, n, sm);
+            trsm_left_lower<T>(n, npk, t.Lsig + t.lsig_off[k], n, Pc, n, sm);
+            predict_column_sums<T>(npk, Pc, n, n, t.yt + o0, -1.0, false, var + (pk - p0), mean + (pk - p0));
+            gemm<T, false, false>((int)Lr, npk, n, (T)-1, t.Bhat + o0 * Lr, Lr, Pc, n, (T)1, t.Bt + pk * Lr, Lr, sm);
         }
         for (int j = L - 1; j >= 0; --j) {
             const long a = anc[j];
@@ -730,18 +757,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_predict(Geom g, DevTree<T> t) {
                 const T* Ga = t.G + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(j * r, np, r, (T)-1, Ga, r, KcB, Lr, (T)1, Bt, Lr, sm);
             }
-            const double* va = t.vpost + a * r;
-            for (int q = threadIdx.x; q < np; q += kThreads) {
-                const T* col = KcB + (long)q * Lr;
-                double ss = 0.0, mm = 0.0;
-                for (int x = 0; x < r; ++x) {
-                    ss += (double)col[x] * (double)col[x];
-                    mm += (double)col[x] * va[x];
-                }
-                var[q] += ss;
-                mean[q] += mm;
-            }
-            __syncthreads();
+            predict_column_sums<T>(np, KcB, Lr, r, t.vpost + a * r, 1.0, true, var, mean);
         }
     }
 }
@@ -833,7 +849,8 @@ void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid,
 }
 template <typename T>
 void launch_predict(const Geom& g, const DevTree<T>& t, int grid, cudaStream_t st) {
-    k_predict<T><<<(unsigned)(t.n_fin < grid ? t.n_fin : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t);
+    const long cnt2 = level_count(t.J, t.M - 2);
+    k_predict<T><<<(unsigned)(cnt2 < grid ? cnt2 : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t);
 }
 template <typename T>
 void launch_reduce(const DevTree<T>& t, double* out, cudaStream_t st) {

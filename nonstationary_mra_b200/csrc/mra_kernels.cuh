@@ -29,7 +29,7 @@ struct DevTree {
     const int64_t* par_order;  // [n_fin_items] finest-kernel work items, most expensive first: a value
                                // v < J^(M-3) is the level M-3 unit v, else the level M-2 group v - J^(M-3)
     long n_fin_items;
-    const int64_t* fin_order;  // [n_fin] finest regions, most expensive prediction work first
+    const int64_t* pred_order; // [J^(M-2)] level M-2 regions (local index), most expensive prediction work first
     const int8_t* factored;    // [n_int] 1: the region's posterior output is kept as F, f
     const int64_t* lsig_off;   // [n_fin+1] offsets of the n_k x n_k blocks
     const int64_t* pc_off;     // [n_fin+1] offsets of the n_k x n_p,k prediction blocks
