@@ -1007,7 +1007,8 @@ mra_status mra_eval_covariance(const mra_model* m, const mra_theta* th, const do
             }
             if (e == cudaSuccess) e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaDeviceSynchronize();
-            if (e == cudaSuccess && n1 * n2) e = cudaMemcpy(out, d, n1 * n2 * sizeof(double), cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess && n1 > 0 && n2 > 0)
+                e = cudaMemcpy(out, d, n1 * n2 * sizeof(double), cudaMemcpyDeviceToHost);
         }
         if (e != cudaSuccess) s = fail(MRA_ERR_CUDA, cudaGetErrorString(e));
     }
