@@ -15,7 +15,7 @@ found so far.  Every proposal is evaluated exactly on the GPU and is accepted
 only if the exact likelihood improves; the new pair joins the training set.
 When proposals stop paying (the box shrinks below ``box_min``), the exact
 optimizer finishes from the best point.  The exact likelihood is therefore
-both the judge of every step and the fallback.
+both the arbiter of every step and the fallback.
 """
 from __future__ import annotations
 
