@@ -97,6 +97,7 @@ RANDOM_CASES = [
     (3, 4, 3, 20, 2500, 30, True, 3, True),      # r = 20, large regions (> 64 rows), nu = 3/2
     (4, 4, 4, 9, 900, 50, False, 1, False),      # stationary
     (5, 2, 7, 4, 700, 80, True, 3, True),        # deep tree
+    (6, 4, 5, 16, 3000, 200, True, 3, True),     # finest work items both batched and split; children up to 230
 ]
 
 
