@@ -607,6 +607,8 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     {
         const long n_units = M >= 3 ? level_count(J, M - 3) : 0;
         const long lvl3 = M >= 3 ? level_start(J, M - 3) : 0;
+        long unit_max = 64L * J;  // observations of a unit processed as one item
+        if (const char* e = std::getenv("MRA_UNIT_OBS_MAX")) unit_max = std::max(0L, std::atol(e));
         auto group_cost = [&](long gl) {
             const double n = (double)(h.sub_hi[lvl2 + gl] - h.sub_lo[lvl2 + gl]);
             return n * (n + 64.0 * L);
@@ -615,7 +617,7 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         if (M >= 3) {
             for (long u = 0; u < n_units; ++u) {
                 const long nu = h.sub_hi[lvl3 + u] - h.sub_lo[lvl3 + u];
-                if (nu <= 64L * J) {
+                if (nu <= unit_max) {
                     double c = 0.0;
                     for (long gl = u * J; gl < u * J + J; ++gl) c += group_cost(gl);
                     items.push_back({c, (int64_t)u});
