@@ -142,7 +142,7 @@ mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 // Host-side description of the tree used for sizing, scheduling and FLOP counts.
 struct HostTree {
     std::vector<int64_t> nfin, npred, obs_off, pred_off, fin_anc, pred_order, lsig_off, pc_off;
-    std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi;
+    std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi, dslot;
     std::vector<int8_t> factored;
 };
 
@@ -368,16 +368,21 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     t.obs_off = idx[0]; t.pred_off = idx[1]; t.fin_anc = idx[2]; t.pred_order = idx[3]; t.lsig_off = idx[4];
     t.pc_off = idx[5]; t.child_lo = idx[6]; t.child_hi = idx[7]; t.par_order = idx[8]; t.sub_lo = idx[9];
     t.sub_hi = idx[10];
+    t.dslot = idx[11];
     t.n_fin_items = (long)h.par_order.size();
     // sizes of the level-parity buffers
     size_t aout_sz[2] = {1, 1}, wout_sz[2] = {1, 1}, F_sz[2] = {1, 1}, f_sz[2] = {1, 1};
     for (int m = 1; m <= M - 2; ++m) {
         const long s0 = level_start(J, m), cnt = level_count(J, m);
-        bool any_dense = false, any_fact = false;
-        for (long q = 0; q < cnt; ++q) (h.factored[s0 + q] ? any_fact : any_dense) = true;
-        if (any_dense) {
-            aout_sz[m & 1] = std::max(aout_sz[m & 1], (size_t)(cnt * n_slices(m) * rr));
-            wout_sz[m & 1] = std::max(wout_sz[m & 1], (size_t)(cnt * m * r));
+        long n_dense = 0;
+        bool any_fact = false;
+        for (long q = 0; q < cnt; ++q) {
+            if (h.factored[s0 + q]) any_fact = true;
+            else ++n_dense;
+        }
+        if (n_dense > 0) {
+            aout_sz[m & 1] = std::max(aout_sz[m & 1], (size_t)(n_dense * n_slices(m) * rr));
+            wout_sz[m & 1] = std::max(wout_sz[m & 1], (size_t)(n_dense * m * r));
         }
         if (any_fact) {
             F_sz[m & 1] = std::max(F_sz[m & 1], (size_t)(c->n_obs * (long)m * r));
@@ -600,6 +605,15 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         }
     }
     for (long i = 0; i < n_int; ++i) h.factored[i] = (h.sub_hi[i] - h.sub_lo[i]) <= c->tf ? 1 : 0;
+    // slot of each dense region among the dense regions of its level: the dense
+    // outputs (A~ slices, w~) of a level are stored compactly
+    h.dslot.assign(n_int, -1);
+    for (int mm = 0; mm <= M - 2; ++mm) {
+        const long s0 = level_start(J, mm), cnt = level_count(J, mm);
+        long k = 0;
+        for (long q = 0; q < cnt; ++q)
+            if (!h.factored[s0 + q]) h.dslot[s0 + q] = k++;
+    }
     // work items of the finest kernel: a level M-3 region with its J sibling
     // groups when it holds at most 64 J observations (conditioning shared by
     // the groups), else each of its groups alone (load balance); for M = 2 the
@@ -652,10 +666,11 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     }
     double* y = c->alloc<double>(n_obs, &ce);
     if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: y"));
-    const std::vector<int64_t>* tabs[11] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.pred_order, &h.lsig_off,
-                                            &h.pc_off, &h.child_lo, &h.child_hi, &h.par_order, &h.sub_lo, &h.sub_hi};
-    int64_t* idx[11];
-    for (int q = 0; q < 11; ++q) {
+    const std::vector<int64_t>* tabs[12] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.pred_order, &h.lsig_off,
+                                            &h.pc_off, &h.child_lo, &h.child_hi, &h.par_order, &h.sub_lo, &h.sub_hi,
+                                            &h.dslot};
+    int64_t* idx[12];
+    for (int q = 0; q < 12; ++q) {
         idx[q] = c->alloc<int64_t>(tabs[q]->size(), &ce);
         if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: index tables"));
         mra_status u = upload(idx[q], tabs[q]->data(), tabs[q]->size() * sizeof(int64_t), c->stream);

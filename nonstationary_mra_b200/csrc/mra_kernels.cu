@@ -278,7 +278,8 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
         __syncthreads();
         trsm_left_lower<T>(r, (int)mr, Lt, r, Gi, r, sm);
     }
-    double* wo = t.wout[m & 1] + loc * mr;
+    const long slot = t.dslot[i];  // compact index among the level's dense regions
+    double* wo = t.wout[m & 1] + slot * mr;
     for (long x = threadIdx.x; x < mr; x += kThreads) {
         double s = 0.0;
         for (int tt = 0; tt < r; ++tt) s += (double)Gi[tt + x * r] * v[tt];
@@ -286,7 +287,7 @@ __device__ __noinline__ void dense_step(const DevTree<T>& t, int m, long i, cons
     }
     // A_out(j, j..m-1) = A(j, j..m-1) - G_j^T G_{j..m-1}: both slice rows are
     // contiguous r x r blocks, one product per j reading A from Aagg
-    T* ao = t.aout[m & 1] + loc * n_slices(m) * rr;
+    T* ao = t.aout[m & 1] + slot * n_slices(m) * rr;
     for (int j = 0; j < m; ++j) {
         T* dst = ao + slice_index(m, j, j) * rr;
         const T* src = Aagg + slice_index(m + 1, j, j) * rr;
@@ -582,7 +583,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
     const int r = t.r;
     const long rr = (long)r * r, mr1 = (long)(m + 1) * r;
     const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
-    const long s1 = level_start(t.J, m + 1);
     const long ns_in = n_slices(m + 1);
     T* ws = t.ws + blockIdx.x * t.ws_stride;
     double* wsd = t.wsd + blockIdx.x * t.wsd_stride;
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
                     }
                     accumulate_factored<T>(t, m, (int)(hi - lo), Fin + lo * mr1, mr1, fin + lo, Aagg, wagg, first, sm);
                 } else {
-                    const long cl = c - s1;
+                    const long cl = t.dslot[c];
                     const T* as = ain + cl * ns_in * rr;
                     const double* wsrc = win + cl * mr1;
                     for (long e = threadIdx.x; e < ns_in * rr; e += kThreads) Aagg[e] = first ? as[e] : Aagg[e] + as[e];

@@ -31,6 +31,7 @@ struct DevTree {
     long n_fin_items;
     const int64_t* pred_order; // [J^(M-2)] level M-2 regions (local index), most expensive prediction work first
     const int8_t* factored;    // [n_int] 1: the region's posterior output is kept as F, f
+    const int64_t* dslot;      // [n_int] slot of a dense region among its level's dense regions (-1: factored)
     const int64_t* lsig_off;   // [n_fin+1] offsets of the n_k x n_k blocks
     const int64_t* pc_off;     // [n_fin+1] offsets of the n_k x n_p,k prediction blocks
     int64_t u_off[kMaxLevels]; // offset of level m's U (= G) blocks, m*r*r per region
@@ -51,8 +52,8 @@ struct DevTree {
     double* dpost;             // [n_int] posterior log-lik terms
     double* dfin;              // [J^(M-2)] finest-level log-lik terms of each sibling group
     int fuse_post;             // 1: the finest-group kernel also runs the level M-2 posterior
-    T* aout[2];                // dense A~ slices of one level, ping-pong by level parity
-    double* wout[2];           // dense w~ of one level
+    T* aout[2];                // dense A~ slices of one level's dense regions (by dslot), ping-pong by level parity
+    double* wout[2];           // dense w~ of one level's dense regions (by dslot)
     T* Fbuf[2];                // factored F of one level: [n_obs][m r]
     double* fbuf[2];           // factored f of one level: [n_obs]
     T* ws;                     // per-CTA workspace (T)
