@@ -343,13 +343,23 @@ def sweep_arm(args):
             cfg = synth.Config(f"sweep-{n}-{M}-{r}", n, M, 4, r, 1, 16384, "uniform", 0.3, 5)
             line = {"metric": "MRA loglik evals/sec (scaling sweep)", "unit": "evals/s", "n": n, "M": M, "r": r,
                     "workload": workload_name(cfg)}
+            with_pred = True
             try:
                 xy, pred, theta, md, st = make_problem(cfg, with_pred=True)
                 ctx = api.Context(st, md)
-            except capi.MRAError as exc:
-                line.update(value=None, infeasible=str(exc)[:200])
-                print(json.dumps(line), flush=True)
-                continue
+            except capi.MRAError:
+                # the prediction buffers (G is as large as U) may not fit where the
+                # log-likelihood alone does
+                torch.cuda.empty_cache()
+                with_pred = False
+                try:
+                    xy, pred, theta, md, st = make_problem(cfg, with_pred=False)
+                    ctx = api.Context(st, md)
+                    line.update(note="prediction buffers do not fit: log-likelihood only")
+                except capi.MRAError as exc:
+                    line.update(value=None, infeasible=str(exc)[:200])
+                    print(json.dumps(line), flush=True)
+                    continue
             try:
                 y = draw_values(ctx, st, cfg.seed + 7)
                 ctx.set_obs_values(y)
@@ -365,12 +375,14 @@ def sweep_arm(args):
                 ms = ctx.timer_stop() / steps
                 stats = ctx.stats()
                 dom = max(stats["launches"], key=lambda l: l["ms"])
-                ctx.predict()
-                ctx.timer_start()
-                ctx.predict()
-                ms_pred = ctx.timer_stop()
+                ms_pred = None
+                if with_pred:
+                    ctx.predict()
+                    ctx.timer_start()
+                    ctx.predict()
+                    ms_pred = ctx.timer_stop()
                 line.update(value=1000.0 / ms, ms_per_eval=ms, loglik=ll, flop_per_eval=stats["flop_last"],
-                            predict_ms=ms_pred, predictions=int(st.n_pred),
+                            predict_ms=ms_pred, predictions=int(st.n_pred) if with_pred else 0,
                             device_gb=stats["bytes_device"] / 1e9,
                             dominant=f"{dom['kernel']}(level {dom['level']})",
                             dominant_tflops=dom["flop"] / (dom["ms"] * 1e-3) / 1e12, fp64_peak_tflops=peak)
