@@ -190,14 +190,21 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's own code on a bounded sample, scaled by FLOPs
+# CPU baseline: the reference's own code (oracle/_ref, built from its sources)
 # ---------------------------------------------------------------------------
-def cpu_sample_config(cfg):
+# Workloads whose reference layout fits in host memory are timed whole (c2: about
+# 15 GB of finest-level A~).  At c3 the reference would hold about 386 GB of A~,
+# so it cannot run; it is reported as unavailable, with a labelled estimate from
+# two smaller samples of the same generator scaled by algorithmic FLOPs.
+REF_RUNS_WHOLE = ("c1", "c2s", "c2")
+
+
+def cpu_sample_config(cfg, shrink_levels):
+    """Same generator and model with 4^k times fewer points and the tree k levels
+    shallower (same mean number of observations per finest region)."""
     from nonstationary_mra_b200 import synth
-    # same generator and model, 1/64 of the points with the tree two levels
-    # shallower (same mean observations per finest region)
-    return synth.Config(cfg.name + "-cpu-sample", cfg.n // 64, cfg.M - 3, cfg.J, cfg.r, cfg.nu_x2, 0, cfg.layout,
-                        cfg.range_sd, cfg.seed + 1000)
+    return synth.Config(f"{cfg.name}-sample{shrink_levels}", cfg.n >> (2 * shrink_levels), cfg.M - shrink_levels,
+                        cfg.J, cfg.r, cfg.nu_x2, 0, cfg.layout, cfg.range_sd, cfg.seed + 1000 + shrink_levels)
 
 
 def canonical_flops(st):
@@ -217,70 +224,128 @@ def canonical_flops(st):
     return float(total)
 
 
-def run_cpu_reference(cfg, reps, warmup, ctx_factory=None):
-    """Times Approximation::likelihood() of the reference (compiled from its own
-    sources, oracle/_ref) on the bounded sample, all host threads.  Falls back to
-    the numpy restatement of the oracle when the reference binary is absent."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def time_reference(cfg, reps):
+    """Approximation::likelihood() of the reference on the whole workload ``cfg``
+    (the partition is built once, outside the timed calls; each call on a fresh
+    Approximation as the reference's optimizer does), all host threads with
+    OpenBLAS single-threaded inside OpenMP.  Observation values come from
+    synth.smooth_values (the reference's work does not depend on them).  Falls
+    back to the numpy restatement of the oracle, single-threaded, when the
+    reference binary is absent.  Returns (seconds per call, kind, cores, n_obs, FLOPs)."""
     from nonstationary_mra_b200 import refio, synth
-    sc = cpu_sample_config(cfg)
-    xy, _, theta, md, st = make_problem(sc)
-    f_sample = canonical_flops(st)
+    xy, _, theta, md, st = make_problem(cfg)
+    flops = canonical_flops(st)
+    y = synth.smooth_values(xy, theta, cfg.seed + 500)
     cores = os.cpu_count() or 1
     tmp = tempfile.mkdtemp(prefix="mra_cpu_")
     try:
-        y = np.zeros(sc.n)
-        if ctx_factory is not None:
-            ctx = ctx_factory(st, md)
-            y_st = draw_values(ctx, st, sc.seed + 7)
-            ctx.close()
-            y[st.obs_index] = y_st
-        synth.write_case(tmp, sc, xy, y, np.zeros((2, 0)), theta)
+        synth.write_case(tmp, cfg, xy, y, np.zeros((2, 0)), theta)
         if os.path.exists(REF_BIN):
             X = refio.parse_parameters(os.path.join(tmp, "ext_parameters"))
             env = dict(os.environ, OMP_NUM_THREADS=str(cores), OPENBLAS_NUM_THREADS="1",
                        **{k: str(v) for k, v in X.items()})
-            res = subprocess.run([REF_BIN, "--reps", str(reps + warmup)], cwd=tmp, env=env, capture_output=True,
-                                 text=True, timeout=1800)
+            res = subprocess.run([REF_BIN, "--reps", str(reps)], cwd=tmp, env=env, capture_output=True,
+                                 text=True, timeout=3600)
             if res.returncode != 0:
                 raise RuntimeError(res.stdout[-1000:] + res.stderr[-1000:])
             secs = [float(tok.split("=")[1]) for line in res.stdout.splitlines() if line.startswith("ORACLE rep=")
                     for tok in line.split() if tok.startswith("likelihood_seconds=")]
-            secs = secs[warmup:]
             kind, used = "reference", cores
         else:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import mra_oracle as oracle
             ost, omd, _ = oracle.load_case(tmp, mode="likelihood")
             secs = []
-            for i in range(reps + warmup):
+            for _ in range(reps):
                 t0 = time.perf_counter()
                 oracle.loglik(ost, omd)
-                if i >= warmup:
-                    secs.append(time.perf_counter() - t0)
+                secs.append(time.perf_counter() - t0)
             kind, used = "port", 1
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
-    return {"secs": secs, "f_sample": f_sample, "kind": kind, "cores": used, "sample": sc, "n_obs": st.n_obs}
+    return secs, kind, used, st.n_obs, flops
+
+
+def reference_estimate(cfg, reps=3):
+    """For a workload the reference cannot hold: the FLOP-scaled projection from a
+    sample 64x smaller (three levels shallower), and the same projection from a
+    sample 256x smaller as a check of the scaling (the two should agree)."""
+    _, _, _, _, st_full = make_problem(cfg)
+    f_full = canonical_flops(st_full)
+    out = {}
+    for k in (4, 3):
+        sc = cpu_sample_config(cfg, k)
+        secs, kind, cores, n_obs, f = time_reference(sc, reps + 1)
+        t = statistics.median(secs[1:])
+        out[k] = {"points": sc.n, "M": sc.M, "seconds": t, "flops": f, "evals_per_s_scaled": f / (f_full * t)}
+    a, b = out[4], out[3]
+    return {"value": b["evals_per_s_scaled"], "unit": "evals/s", "kind": kind, "cores": cores,
+            "method": (f"likelihood() of a {b['points']}-point M={b['M']} sample of the same generator "
+                       f"(median {b['seconds']:.3f} s) scaled by algorithmic FLOPs ({f_full:.3e} / {b['flops']:.3e})"),
+            "scaling_check": {"sample_points": [a["points"], b["points"]], "sample_M": [a["M"], b["M"]],
+                              "seconds": [a["seconds"], b["seconds"]], "flops": [a["flops"], b["flops"]],
+                              "time_ratio": b["seconds"] / a["seconds"], "flop_ratio": b["flops"] / a["flops"]},
+            "cpu": cpu_model()}
+
+
+def cpu_baseline_for(cfg, reps):
+    """cpu_baseline object of the line: the whole workload where the reference
+    fits in host memory, else the labelled FLOP-scaled estimate."""
+    if cfg.name in REF_RUNS_WHOLE:
+        secs, kind, cores, n_obs, _ = time_reference(cfg, reps + 1)
+        t = statistics.median(secs[1:]) if len(secs) > 1 else secs[0]
+        return {"value": 1.0 / t, "unit": "evals/s", "cores": cores, "kind": kind, "same_config": True,
+                "cpu": cpu_model(),
+                "sample": (f"the whole {cfg.name} workload ({n_obs} observations): median of {len(secs) - 1} "
+                           f"likelihood() calls after one untimed call = {t:.3f} s")}
+    est = reference_estimate(cfg)
+    return {"value": est["value"], "unit": "evals/s", "cores": est["cores"], "kind": est["kind"],
+            "same_config": False, "cpu": est["cpu"], "estimate": True,
+            "sample": ("ESTIMATE: the reference cannot hold this workload (about 386 GB of finest-level A~ "
+                       "in its layout); " + est["method"]), "scaling_check": est["scaling_check"]}
 
 
 def reference_arm(args):
     from nonstationary_mra_b200 import synth
     cfg = synth.CONFIGS[args.config]
-    _, _, _, _, st_full = make_problem(cfg)
-    f_full = canonical_flops(st_full)
-    r = run_cpu_reference(cfg, max(args.steps, 1), max(args.warmup, 0))
-    t = statistics.median(r["secs"])
-    value = 1.0 / (t * f_full / r["f_sample"])
-    sc = r["sample"]
-    sample = (f"{sc.n} points, M={sc.M}, J={sc.J}, r={sc.r} (same generator), one likelihood() per step, "
-              f"scaled to the {cfg.name} workload by algorithmic FLOPs ({f_full:.3e} / {r['f_sample']:.3e})")
-    line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": len(r["secs"]),
-            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(cfg), "parallelism": "cpu", "sample_seconds_median": t},
-            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": r["cores"], "kind": r["kind"],
-                             "sample": sample},
-            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    base = {"metric": METRIC, "unit": "evals/s", "n_gpus": args.gpus, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(cfg), "parallelism": "cpu"}}
+    if cfg.name not in REF_RUNS_WHOLE:
+        est = reference_estimate(cfg)
+        line = dict(base, value=None, steps=0, warmup=0, ms_per_step=None,
+                    unavailable=(f"the reference's layout needs about 386 GB of host memory for the finest-level "
+                                 f"A~ at {cfg.name} and one likelihood() would take minutes; "
+                                 f"see 'estimate' and 'bench.py --config c2 --impl reference' for a measured "
+                                 f"same-config comparison"),
+                    estimate=est,
+                    cpu_baseline={"value": None, "unit": "evals/s", "cores": est["cores"], "kind": est["kind"],
+                                  "sample": "not run: " + est["method"]},
+                    e2e={"value": None, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(line))
+        return
+    steps, warmup = max(args.steps, 1), max(args.warmup, 0)
+    secs, kind, cores, n_obs, _ = time_reference(cfg, steps + warmup)
+    secs = secs[warmup:]
+    t = statistics.median(secs)
+    value = 1.0 / t
+    line = dict(base, value=value, steps=len(secs), warmup=warmup, ms_per_step=1000.0 * t,
+                cpu_baseline={"value": value, "unit": "evals/s", "cores": cores, "kind": kind, "same_config": True,
+                              "cpu": cpu_model(),
+                              "sample": (f"the whole {cfg.name} workload ({n_obs} observations), one likelihood() "
+                                         f"per step; median of {len(secs)}")},
+                e2e={"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    line["config"]["seconds_per_step"] = secs
     print(json.dumps(line))
 
 
@@ -552,15 +617,7 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
-            r = run_cpu_reference(cfg, 3, 1, ctx_factory=lambda s, m: api.Context(s, m))
-            t = statistics.median(r["secs"])
-            f_full = canonical_flops(st)  # the reference algorithm's work, as in the reference arm
-            sc = r["sample"]
-            cpu = {"value": 1.0 / (t * f_full / r["f_sample"]), "unit": "evals/s", "cores": r["cores"],
-                   "kind": r["kind"],
-                   "sample": (f"{sc.n} points, M={sc.M}, J={sc.J}, r={sc.r} (same generator): median of "
-                              f"{len(r['secs'])} likelihood() runs = {t:.3f} s, scaled to this workload by "
-                              f"algorithmic FLOPs ({f_full:.3e} / {r['f_sample']:.3e})")}
+            cpu = cpu_baseline_for(cfg, 2)
         except Exception as exc:  # reported, never silently replaced
             cpu = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {exc}"[:300]}

@@ -216,9 +216,14 @@ mra_status mra_timer_stop(mra_ctx* ctx, double* ms);
  * device-wide synchronisation of cudaMalloc/cudaFree on every call.  Inputs and
  * output are the caller's DEVICE buffers: p1_dev [3][n1] and p2_dev [3][n2]
  * coordinates, out_dev n1*n2 doubles (n1*n1 when self != 0; p2_dev/n2 ignored).
- * The model's basis tables and theta are read from host memory as elsewhere.
- * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default stream)
- * and the call returns without waiting for it.
+ * The model's basis tables and theta are read from host memory as elsewhere,
+ * with cudaMemcpyAsync on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream): theta always goes through a pageable buffer of the call, and a copy
+ * from pageable memory waits for the stream's earlier work before it starts.
+ * Basis tables or weights in pinned (page-locked) host memory are copied
+ * asynchronously instead, so they must stay unchanged until the stream has
+ * passed this call.  The kernels are queued on `stream`; the call does not wait
+ * for them.
  *
  * Scratch lives in one fixed array in device global memory, held by every GPU
  * that loads the library until the process exits; limits: n1 + n2 <=

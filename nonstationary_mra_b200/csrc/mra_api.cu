@@ -119,7 +119,9 @@ Geom make_geom(const mra_model* m) {
     return g;
 }
 
-mra_status check_model(const mra_model* m) {
+}  // namespace
+
+mra_status mra::check_model(const mra_model* m) {
     if (!m) return fail(MRA_ERR_ARG, "model is NULL");
     if (m->distance < 0 || m->distance > 2) return fail(MRA_ERR_ARG, "unknown distance kind");
     if (m->nu_x2 != 1 && m->nu_x2 != 3) return fail(MRA_ERR_ARG, "nu must be 1/2 or 3/2");
@@ -132,6 +134,8 @@ mra_status check_model(const mra_model* m) {
     }
     return MRA_OK;
 }
+
+namespace {
 
 mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
     if (bytes == 0) return MRA_OK;

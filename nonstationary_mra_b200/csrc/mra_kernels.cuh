@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/mra_b200.h"
 #include "mra_device.cuh"
 
 namespace mra {
@@ -98,6 +99,10 @@ struct FieldParams {
 
 // Sets the text returned by mra_last_error() on this thread.
 void set_last_error(const char* msg);
+
+// Validates a model description (kinds in range, positive basis length and
+// non-NULL basis tables for nonstationary fields); sets the error text.
+mra_status check_model(const mra_model* m);
 
 // Opts the region kernels into their dynamic shared memory size on the current
 // device; call before the first launch (and before any stream capture).

@@ -72,10 +72,11 @@ extern "C" mra_status mra_eval_covariance_static(const mra_model* m, const mra_t
                                                  double* out_dev, void* stream) {
     if (!m || !th || !p1_dev || !out_dev || (!self && !p2_dev))
         return static_fail(MRA_ERR_ARG, "mra_eval_covariance_static: NULL argument");
-    if (m->distance < 0 || m->distance > 2 || (m->nu_x2 != 1 && m->nu_x2 != 3) || (m->basis != 0 && m->basis != 1))
-        return static_fail(MRA_ERR_ARG, "mra_eval_covariance_static: invalid model");
+    if (mra_status ms = check_model(m)) return ms;
     if (self) n2 = 0;
-    if (n1 + n2 > (uint64_t)MRA_STATIC_MAX_POINTS)
+    // each count on its own first, so that the sum below cannot wrap around
+    if (n1 > (uint64_t)MRA_STATIC_MAX_POINTS || n2 > (uint64_t)MRA_STATIC_MAX_POINTS ||
+        n1 + n2 > (uint64_t)MRA_STATIC_MAX_POINTS)
         return static_fail(MRA_ERR_ARG,
                            "mra_eval_covariance_static: n1 + n2 exceeds MRA_STATIC_MAX_POINTS (32768 points)");
     for (int f = 0; f < 3; ++f)

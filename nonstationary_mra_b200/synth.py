@@ -105,6 +105,45 @@ def theta_from_vector(v: np.ndarray) -> dict:
     return {"log_sigma": v[:9], "log_range": v[9:18], "log_tausq": float(v[18])}
 
 
+def log_sigma2_at(theta: dict, xy: np.ndarray) -> np.ndarray:
+    """log sigma^2(s) of the synthetic model at points (2, n)."""
+    c = rbf_centers()
+    d2 = (xy[0][:, None] - c[0][None, :]) ** 2 + (xy[1][:, None] - c[1][None, :]) ** 2
+    return 2.0 * (np.exp(-d2 / (2 * RBF_WIDTH ** 2)) @ np.asarray(theta["log_sigma"], dtype=np.float64))
+
+
+def smooth_values(xy: np.ndarray, theta: dict, seed: int, n_features: int = 512, length: float = 0.1,
+                  quantum: float = 2.0 ** -20) -> np.ndarray:
+    """Observation values without the MRA prior: sigma(s) times a random
+    Fourier-feature draw of a Gaussian field of length scale ``length``, plus
+    N(0, tau^2) noise, rounded to multiples of ``quantum``.
+
+    It is vectorised (seconds at n = 262,144) and its output is exactly
+    reproducible across machines: the rounding absorbs last-bit differences of
+    the vectorised cos/exp of different CPUs, so a run elsewhere gets bitwise the
+    same values (callers check a digest)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    omega = rng.standard_normal((2, n_features)) / length
+    phase = rng.uniform(0.0, 2.0 * np.pi, n_features)
+    amp = rng.standard_normal(n_features) * np.sqrt(2.0 / n_features)
+    noise = rng.standard_normal(xy.shape[1])
+    g = np.empty(xy.shape[1])
+    for s in range(0, xy.shape[1], 8192):       # bounded temporaries
+        blk = xy[:, s:s + 8192]
+        g[s:s + 8192] = np.cos(blk.T @ omega + phase) @ amp
+    y = np.exp(0.5 * log_sigma2_at(theta, xy)) * g + np.sqrt(np.exp(theta["log_tausq"])) * noise
+    return np.round(y / quantum) * quantum
+
+
+def digest(*arrays) -> str:
+    """Short SHA-256 of float64 arrays: proves two runs saw the same inputs."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()[:16]
+
+
 def write_case(case_dir: str, cfg: Config, xy: np.ndarray, values: np.ndarray, pred: np.ndarray, theta: dict,
                mode: str = "likelihood") -> None:
     """user_parameters + ext_parameters + binary files for a config."""

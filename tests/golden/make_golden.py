@@ -23,6 +23,7 @@ Observation values are drawn from the MRA prior with the numpy oracle
 (oracle/mra_oracle.sample_prior) from PCG64-seeded normals.
 
     python tests/golden/make_golden.py [--only NAME]
+    python tests/golden/make_golden.py --large [--only NAME]   # r = 64 cases, see large_cases.py
 """
 from __future__ import annotations
 
@@ -43,8 +44,10 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import mra_oracle as oracle  # noqa: E402
 from nonstationary_mra_b200 import refio, synth  # noqa: E402
 
-REF_EXAMPLE = "/root/reference/data/minimal_reproducible_example"
-REF_PARAMS = "/root/reference/user_parameters"
+# the reference checkout (read only); override with MRA_REFERENCE=/path/to/nonstationary_mra
+REFERENCE = os.environ.get("MRA_REFERENCE", "/root/reference")
+REF_EXAMPLE = os.path.join(REFERENCE, "data", "minimal_reproducible_example")
+REF_PARAMS = os.path.join(REFERENCE, "user_parameters")
 MRA_REF = os.path.join(ROOT, "oracle", "_ref", "mra_ref")
 MRA_REF_EXT = os.path.join(ROOT, "oracle", "_ref", "mra_ref_ext")
 
@@ -106,20 +109,29 @@ def resample_values(d, seed):
     refio.write_data(path, lon, lat, new, reg)
 
 
-def run_reference(d, mode):
+def run_reference(d, mode, threads=4, pred_npz=False, inputs=None):
+    """Runs the reference build on the case in ``d`` (or, for the regenerated
+    cases, on ``inputs(tmp)`` written into the scratch directory) and returns
+    its ORACLE values."""
     ext = os.path.exists(os.path.join(d, "ext_parameters"))
-    env = dict(os.environ, OMP_NUM_THREADS="4", OPENBLAS_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OPENBLAS_NUM_THREADS="1")
     if ext:
         X = refio.parse_parameters(os.path.join(d, "ext_parameters"))
         env.update({k: str(v) for k, v in X.items()})
     with tempfile.TemporaryDirectory() as tmp:
-        for f in os.listdir(d):
-            shutil.copy(os.path.join(d, f), tmp)
+        if inputs is not None:
+            inputs(tmp)
+            ext = True
+            X = refio.parse_parameters(os.path.join(tmp, "ext_parameters"))
+            env.update({k: str(v) for k, v in X.items()})
+        else:
+            for f in os.listdir(d):
+                shutil.copy(os.path.join(d, f), tmp)
         P = refio.parse_parameters(os.path.join(tmp, "user_parameters"))
         P["CALCULATION_MODE"] = mode
         refio.write_parameters(os.path.join(tmp, "user_parameters"), P)
         res = subprocess.run([MRA_REF_EXT if ext else MRA_REF], cwd=tmp, env=env, capture_output=True, text=True,
-                             timeout=3600)
+                             timeout=4 * 3600)
         if res.returncode != 0:
             raise RuntimeError(f"reference failed on {d}:\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
         out = {}
@@ -129,7 +141,12 @@ def run_reference(d, mode):
                     k, v = tok.split("=")
                     out[k] = float(v)
         if mode == "prediction":
-            shutil.copy(os.path.join(tmp, P["PREDICTION_RESULTS_FILE_NAME"]), os.path.join(d, "pred_golden.bin"))
+            dump = os.path.join(tmp, P["PREDICTION_RESULTS_FILE_NAME"])
+            if pred_npz:
+                _, _, mean, var = refio.read_prediction_dump(dump)
+                np.savez(os.path.join(d, "pred_golden.npz"), mean=mean, var=var)
+            else:
+                shutil.copy(dump, os.path.join(d, "pred_golden.bin"))
         return out
 
 
@@ -202,8 +219,39 @@ CASES = {"example": case_example, "ref_prog_j4": case_ref_prog_j4, "ref_gc_j2": 
          "ref_stationary": case_ref_stationary, "ext_mix": case_ext_mix, "ext_nu32": case_ext_nu32, "c1": case_c1}
 
 
+def make_large(name, threads):
+    """A regenerated r = 64 case (tests/golden/large_cases.py): only the spec with
+    the input digests, the reference's outputs and its predictions are kept."""
+    import platform
+    import large_cases
+    d = os.path.join(HERE, name)
+    os.makedirs(d, exist_ok=True)
+    cfg = large_cases.SPECS[name]
+    dig = {}
+    lk = run_reference(d, "likelihood", threads, inputs=lambda tmp: dig.update(large_cases.write_inputs(tmp, name)))
+    pr = run_reference(d, "prediction", threads, pred_npz=True,
+                       inputs=lambda tmp: large_cases.write_inputs(tmp, name, "prediction"))
+    spec = {"config": cfg.__dict__, "generator": "tests/golden/large_cases.py:generate", "digests": dig}
+    with open(os.path.join(d, "spec.json"), "w") as f:
+        json.dump(spec, f, indent=1)
+    g = {"d": lk["d"], "loglik": lk["loglik"], "n_obs": int(lk["n_obs"]),
+         "likelihood_seconds": lk["likelihood_seconds"], "predict_seconds": pr["predict_seconds"],
+         "threads": threads, "cpu": platform.processor() or platform.machine()}
+    with open(os.path.join(d, "golden.json"), "w") as f:
+        json.dump(g, f, indent=1)
+    print(name, g)
+
+
 def main():
     only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
+    if "--large" in sys.argv:
+        sys.path.insert(0, HERE)
+        import large_cases
+        threads = os.cpu_count() or 4
+        for name in large_cases.SPECS:
+            if not only or name == only:
+                make_large(name, threads)
+        return
     for name, fn in CASES.items():
         if only and name != only:
             continue
