@@ -465,41 +465,66 @@ def sweep_arm(args):
 def predict_arm(args):
     """Prediction throughput: the workload's prediction points resident with the
     tree; one step = log-likelihood with the predictive factors kept + the
-    prediction of every point (the reference's likelihood() + predict()).
-    Reports predictions/s of the whole step and of the prediction launch
-    alone (CUDA events on the library's stream)."""
+    prediction of every point (the reference's likelihood() + predict()),
+    replayed from one captured CUDA graph.  Reports predictions/s of the whole
+    step and of the prediction launch alone (CUDA events on the library's
+    stream), and the other precision on the same inputs with its error per
+    output against the FP64 path."""
     from nonstationary_mra_b200 import api, capi, synth
     cfg = synth.CONFIGS[args.config]
     line = {"metric": "MRA predictions/sec (likelihood + predict)", "unit": "predictions/s",
-            "workload": workload_name(cfg), "n_pred": cfg.n_pred}
+            "workload": workload_name(cfg), "n_pred": cfg.n_pred, "precision": args.precision,
+            "cuda_graph": not args.no_graph}
     try:
         xy, pred, theta, md, st = make_problem(cfg, with_pred=True)
-        ctx = api.Context(st, md)
     except capi.MRAError as exc:
         line.update(value=None, infeasible=str(exc)[:200])
         print(json.dumps(line), flush=True)
         return
+    y = None
+
+    def run(precision):
+        nonlocal y
+        ctx = api.Context(st, md, precision=precision)
+        try:
+            if y is None:
+                y = draw_values(ctx, st, cfg.seed + 7)
+            ctx.set_obs_values(y)
+            ctx.set_theta()
+            for _ in range(max(args.warmup, 1)):
+                ctx.predict()
+            if not args.no_graph:
+                ctx.capture_graph()
+                ctx.predict()
+            steps = max(args.steps, 1)
+            ctx.timer_start()
+            for _ in range(steps):
+                mean, var = ctx.predict()
+            ms = ctx.timer_stop() / steps
+            stats = ctx.stats()
+            ms_kernel = sum(l["ms"] for l in stats["launches"] if l["kernel"] == "predict")
+            return {"ms": ms, "ms_kernel": ms_kernel, "mean": mean, "var": var, "gb": stats["bytes_device"] / 1e9,
+                    "steps": steps}
+        finally:
+            ctx.close()
+
     try:
-        y = draw_values(ctx, st, cfg.seed + 7)
-        ctx.set_obs_values(y)
-        ctx.set_theta()
-        for _ in range(max(args.warmup, 1)):
-            ctx.predict()
-        steps = max(args.steps, 1)
-        ctx.timer_start()
-        for _ in range(steps):
-            mean, var = ctx.predict()
-        ms = ctx.timer_stop() / steps
-        stats = ctx.stats()
-        ms_kernel = sum(l["ms"] for l in stats["launches"] if l["kernel"] == "predict")
-        line.update(value=st.n_pred / (ms * 1e-3), ms_per_step=ms, predict_launch_ms=ms_kernel,
-                    predict_launch_per_s=st.n_pred / (ms_kernel * 1e-3) if ms_kernel > 0 else None,
-                    device_gb=stats["bytes_device"] / 1e9, mean_abs=float(np.mean(np.abs(mean))),
-                    steps=steps, warmup=args.warmup)
+        a = run(args.precision)
+        line.update(value=st.n_pred / (a["ms"] * 1e-3), ms_per_step=a["ms"], predict_launch_ms=a["ms_kernel"],
+                    predict_launch_per_s=st.n_pred / (a["ms_kernel"] * 1e-3) if a["ms_kernel"] > 0 else None,
+                    device_gb=a["gb"], mean_abs=float(np.mean(np.abs(a["mean"]))), steps=a["steps"],
+                    warmup=args.warmup)
+        if not args.no_compare:
+            oprec = "mixed" if args.precision == "fp64" else "fp64"
+            b = run(oprec)
+            f64, mix = (a, b) if args.precision == "fp64" else (b, a)
+            err = lambda u, v: float(np.max(np.abs(u - v) / np.maximum(1.0, np.abs(v))))
+            line["other_precision"] = {
+                "precision": oprec, "ms_per_step": b["ms"], "predict_launch_ms": b["ms_kernel"],
+                "mixed_err_vs_fp64": {"mean": err(mix["mean"], f64["mean"]), "var": err(mix["var"], f64["var"])},
+                "mixed_speedup_vs_fp64": f64["ms"] / mix["ms"]}
     except capi.MRAError as exc:
         line.update(value=None, failed=str(exc)[:200])
-    finally:
-        ctx.close()
     print(json.dumps(line), flush=True)
 
 

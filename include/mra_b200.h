@@ -164,7 +164,12 @@ mra_status mra_loglik(mra_ctx* ctx, double* d_out, double* loglik_out);
  * order of dump_prediction_result, class_approximation.cpp:493-535). */
 mra_status mra_predict(mra_ctx* ctx, double* mean, double* var);
 
-/* Captures prior->posterior into a CUDA graph; later mra_loglik calls replay it. */
+/* Captures the evaluation into CUDA graphs: prior -> posterior, which later
+ * mra_loglik calls replay, and, when the structure has prediction locations,
+ * prior -> posterior (predictive factors kept) -> prediction, which later
+ * mra_predict calls replay.  theta and the observation values are read from
+ * device memory by the captured kernels, so mra_set_theta / mra_set_obs_values
+ * between replays need no recapture. */
 mra_status mra_capture_graph(mra_ctx* ctx);
 
 mra_status mra_get_stats(const mra_ctx* ctx, mra_stats* out);

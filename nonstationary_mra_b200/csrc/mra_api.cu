@@ -69,6 +69,10 @@ struct mra_ctx {
     int n_timed = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // prior -> posterior (predictive factors kept) -> prediction, when the
+    // structure has prediction locations
+    cudaGraph_t graph_pred = nullptr;
+    cudaGraphExec_t graph_pred_exec = nullptr;
     double* d_theta = nullptr;  // 16 doubles
     double* d_weights[3]{};
     long nb[3]{};
@@ -97,6 +101,8 @@ struct mra_ctx {
     ~mra_ctx() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
+        if (graph_pred_exec) cudaGraphExecDestroy(graph_pred_exec);
+        if (graph_pred) cudaGraphDestroy(graph_pred);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : tev)
@@ -814,9 +820,14 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
 mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     if (!c) return fail(MRA_ERR_ARG, "NULL context");
     if (!c->have_pred) return fail(MRA_ERR_STATE, "the structure has no prediction locations");
-    mra_status s = run_eval(c, true);
-    if (s) return s;
-    s = finish_eval(c);
+    if (c->graph_pred_exec) {
+        CU(cudaGraphLaunch(c->graph_pred_exec, c->stream));
+        c->stats.graph_replays++;
+    } else {
+        mra_status s = run_eval(c, true);
+        if (s) return s;
+    }
+    mra_status s = finish_eval(c);
     if (s) return s;
     const double* dm = c->td.mean;
     const double* dv = c->td.var;
@@ -825,11 +836,13 @@ mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     return MRA_OK;
 }
 
-mra_status mra_capture_graph(mra_ctx* c) {
-    if (!c) return fail(MRA_ERR_ARG, "NULL context");
-    if (c->graph_exec) return MRA_OK;
+namespace {
+
+// Captures one evaluation sequence (log-likelihood, or log-likelihood with the
+// predictive factors kept followed by prediction) from the context's stream.
+mra_status capture_one(mra_ctx* c, bool predict, cudaGraph_t* graph, cudaGraphExec_t* exec) {
     CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    mra_status s = run_eval(c, false);
+    mra_status s = run_eval(c, predict);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (s) {
@@ -837,8 +850,28 @@ mra_status mra_capture_graph(mra_ctx* c) {
         return s;
     }
     if (e != cudaSuccess) return fail(MRA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    c->graph = g;
-    CU(cudaGraphInstantiate(&c->graph_exec, g, 0));
+    cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        *exec = nullptr;
+        return fail(MRA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    *graph = g;
+    return MRA_OK;
+}
+
+}  // namespace
+
+mra_status mra_capture_graph(mra_ctx* c) {
+    if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (!c->graph_exec) {
+        mra_status s = capture_one(c, false, &c->graph, &c->graph_exec);
+        if (s) return s;
+    }
+    if (c->have_pred && !c->graph_pred_exec) {
+        mra_status s = capture_one(c, true, &c->graph_pred, &c->graph_pred_exec);
+        if (s) return s;
+    }
     return MRA_OK;
 }
 

@@ -163,6 +163,32 @@ def test_graph_replay_and_theta_updates():
     ctx.close()
 
 
+def test_prediction_graph_replay():
+    """prior -> posterior -> predict captured in one graph: replays give bitwise
+    the eager results, and follow theta changes without recapture."""
+    st, md = random_case(13, 4, 4, 16, 1500, 120, clustered=True)
+    ctx = api.Context(st, md)
+    ctx.set_theta(range_scale=1.0)
+    m0, v0 = ctx.predict()
+    ctx.capture_graph()
+    replays = ctx.stats()["graph_replays"]
+    m1, v1 = ctx.predict()
+    assert ctx.stats()["graph_replays"] == replays + 1
+    assert np.array_equal(m0, m1) and np.array_equal(v0, v1)
+    ctx.set_theta(range_scale=0.8)
+    m2, v2 = ctx.predict()
+    ost, omd = to_oracle(st, md)
+    omd.range_scale = 0.8
+    m_ref, v_ref = oracle.predict(ost, omd)
+    assert not np.array_equal(m2, m0)
+    assert close_pred(m2, m_ref) and close_pred(v2, v_ref)
+    # the log-likelihood graph is still the one mra_loglik replays
+    d, _ = ctx.loglik()
+    d_ref, _ = oracle.loglik(ost, omd)
+    assert abs(d - d_ref) <= LL_RTOL * max(1.0, abs(d_ref))
+    ctx.close()
+
+
 def test_autotune_keeps_results_bitwise():
     st, md = random_case(12, 4, 4, 16, 1500, 10, clustered=True)
     ctx, (d0, _) = run_loglik(st, md)
