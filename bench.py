@@ -76,6 +76,10 @@ def parse_args():
     p.add_argument("--predict", action="store_true",
                    help="instead of the log-likelihood line: prediction throughput on the workload with its "
                         "prediction points (log-likelihood with the predictive factors kept, then prediction)")
+    p.add_argument("--mixed-report", action="store_true",
+                   help="instead of the log-likelihood line: the mixed path against the FP64 path on the same "
+                        "inputs, per stage (device time of each launch, error of each part of d), with the "
+                        "observed values and with y = 0 (log-determinants alone)")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -528,8 +532,57 @@ def predict_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def mixed_report_arm(args):
+    """Attribution of the mixed path's error and time, stage by stage, on the
+    device: both precisions evaluate the same tree and values; for every launch
+    its CUDA-event time, and for every part of d (posterior terms of each interior
+    level; finest-level terms with the level M-2 posterior) the mixed path's
+    difference from FP64.  Repeated with y = 0, where d is the log-determinants
+    alone, to separate them from the quadratic forms."""
+    from nonstationary_mra_b200 import api, synth
+    cfg = synth.CONFIGS[args.config]
+    xy, pred, theta, md, st = make_problem(cfg)
+    out = {"metric": "mixed-path attribution", "workload": workload_name(cfg), "M": cfg.M}
+    runs = {}
+    y = None
+    for prec in ("fp64", "mixed"):
+        ctx = api.Context(st, md, precision=prec)
+        if y is None:
+            y = draw_values(ctx, st, cfg.seed + 7)
+        res = {}
+        for label, vals in (("y", y), ("y0", np.zeros_like(y))):
+            ctx.set_obs_values(vals)
+            ctx.set_theta()
+            for _ in range(max(args.warmup, 1)):
+                ctx.loglik()
+            d, ll = ctx.loglik()
+            stats = ctx.stats()
+            res[label] = {"d": d, "loglik": ll, "terms": ctx.terms().tolist(),
+                          "launches": [(l["kernel"], l["level"], l["ms"]) for l in stats["launches"]],
+                          "ms_total": stats["ms_total"]}
+        ctx.close()
+        runs[prec] = res
+    for label in ("y", "y0"):
+        a, b = runs["fp64"][label], runs["mixed"][label]
+        parts = []
+        for m in range(cfg.M):
+            name = f"posterior terms, level {m}" if m < cfg.M - 1 else "finest terms + level M-2 posterior"
+            parts.append({"part": name, "fp64": a["terms"][m], "mixed_minus_fp64": b["terms"][m] - a["terms"][m]})
+        out[label] = {"d_fp64": a["d"], "d_mixed": b["d"], "d_rel_err": abs(b["d"] - a["d"]) / abs(a["d"]),
+                      "loglik_fp64": a["loglik"], "loglik_mixed": b["loglik"],
+                      "loglik_rel_err": abs(b["loglik"] - a["loglik"]) / abs(a["loglik"]), "parts": parts}
+    la = runs["fp64"]["y"]["launches"]
+    lb = runs["mixed"]["y"]["launches"]
+    out["launch_ms"] = {"fp64": la, "mixed": lb, "fp64_total": runs["fp64"]["y"]["ms_total"],
+                        "mixed_total": runs["mixed"]["y"]["ms_total"]}
+    print(json.dumps(out))
+
+
 def main():
     args = parse_args()
+    if args.mixed_report:
+        mixed_report_arm(args)
+        return
     if args.fit:
         fit_arm(args)
         return

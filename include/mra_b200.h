@@ -174,6 +174,15 @@ mra_status mra_capture_graph(mra_ctx* ctx);
 
 mra_status mra_get_stats(const mra_ctx* ctx, mra_stats* out);
 
+/* Diagnostics, no counterpart in the reference: the parts of d (the reference's
+ * internal loglikelihood) from the last evaluation, by where they are computed.
+ * out[m], m = 0..M-2: sum over the level-m regions of their posterior terms
+ * (-2 log|L_i| + 2 log|L~_i| - v_i^T v_i, or the factored form's equal);
+ * out[M-1]: the finest-level terms (y~^T y~ + 2 log|L_Sigma|) together with the
+ * level M-2 posterior terms, which one kernel computes.  sum(out) = d up to
+ * summation order.  n_out >= M.  Waits for the context's stream. */
+mra_status mra_get_terms(mra_ctx* ctx, double* out, int32_t n_out);
+
 /* Draws y from the MRA prior at the current theta:
  * y = sum_j U_{obs,j}^T z_{a_j} + L_Sigma z_k, z_interior [n_interior*r],
  * z_obs [n_obs] standard normals given by the caller (host memory). */

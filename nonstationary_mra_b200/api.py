@@ -54,6 +54,7 @@ class Context:
         st.finest_parent, st.knots, st.obs_offset = u64p(parent), f64p(knots), u64p(obs_off)
         st.obs, st.obs_value = f64p(obs), f64p(y)
         self.n_obs = int(y.shape[0])
+        self.M = int(structure.M)
         self.n_pred = 0
         if getattr(structure, "pred_offset", None) is not None:
             poff = _c(structure.pred_offset, np.uint64)
@@ -156,6 +157,13 @@ class Context:
         n = s.n_timed
         out["launches"] = [{"kernel": capi.KERNEL_NAMES.get(s.timed_kind[i], "?"), "level": s.timed_level[i],
                             "ms": s.timed_ms[i], "flop": s.timed_flop[i]} for i in range(n)]
+        return out
+
+    def terms(self) -> np.ndarray:
+        """Parts of d from the last evaluation: [m] = level-m posterior terms for
+        m < M-1, [M-1] = finest-level plus level M-2 terms (mra_get_terms)."""
+        out = np.zeros(self.M)
+        check(self._lib.mra_get_terms(self._h, f64p(out), self.M), "mra_get_terms")
         return out
 
     def close(self):

@@ -73,6 +73,8 @@ struct mra_ctx {
     // structure has prediction locations
     cudaGraph_t graph_pred = nullptr;
     cudaGraphExec_t graph_pred_exec = nullptr;
+    int graph_timed[2] = {0, 0};     // timed stages of the log-likelihood / prediction graph
+    int graph_launches[2] = {0, 0};  // kernels launched by each
     double* d_theta = nullptr;  // 16 doubles
     double* d_weights[3]{};
     long nb[3]{};
@@ -264,31 +266,37 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     CU(cudaMemsetAsync(td.err, 0, 4 * sizeof(int), st));
     const long np_all = c->n_int * c->r + c->n_obs + c->n_pred;
     const long rr = (long)c->r * c->r;
-    int i = 0;
+    int i = 0, launched = 0;
     for (const auto& l : c->plan) {
         CU(record(c->tev[2 * i], st, capturing));
         switch (l.kind) {
             case MRA_KERNEL_FIELDS:
                 launch_fields(c->geom, c->fp, td.pts.c0, td.pts.c1, td.pts.c2, np_all, const_cast<double*>(td.pts.s2),
                               const_cast<double*>(td.pts.beta), const_cast<double*>(td.pts.t2), st);
+                launched += 1;
                 break;
             case MRA_KERNEL_PRIOR_LEVEL:
-                if (mixed) launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
-                else launch_prior_level<double>(c->geom, td, l.level, c->grid, st);
+                if (mixed) launched += launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
+                else launched += launch_prior_level<double>(c->geom, td, l.level, c->grid, st);
                 break;
             case MRA_KERNEL_FINEST:
-                if (mixed) launch_finest_group<float>(c->geom, tf, c->grid, predict, st);
-                else launch_finest_group<double>(c->geom, td, c->grid, predict, st);
+                if (mixed) launched += launch_finest_group<float>(c->geom, tf, c->grid, predict, st);
+                else launched += launch_finest_group<double>(c->geom, td, c->grid, predict, st);
                 break;
             case MRA_KERNEL_CONVERT:
                 launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
                 launch_convert<float, double>(tf.Pinv, td.Pinv, c->n_int * rr, st);
                 launch_convert<float, double>(tf.Bhat, td.Bhat, c->n_obs * (long)c->L * c->r, st);
+                launched += 3;
                 break;
             case MRA_KERNEL_POSTERIOR_LEVEL:
                 launch_posterior_level<double>(c->geom, td, l.level, c->grid, predict, st);
+                launched += 1;
                 break;
-            case MRA_KERNEL_REDUCE: launch_reduce<double>(td, c->d_result, st); break;
+            case MRA_KERNEL_REDUCE:
+                launch_reduce<double>(td, c->d_result, st);
+                launched += 1;
+                break;
         }
         CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
@@ -299,15 +307,17 @@ mra_status run_eval(mra_ctx* c, bool predict) {
             launch_convert<double, float>(td.Lpost, tf.Lpost, c->n_int * rr, st);
             launch_convert<double, float>(td.G, tf.G, c->u_total, st);
             launch_predict<float>(c->geom, tf, c->grid, st);
+            launched += 3;
         } else {
             launch_predict<double>(c->geom, td, c->grid, st);
+            launched += 1;
         }
         CU(record(c->tev[2 * i + 1], st, capturing));
         ++i;
     }
     CU(cudaGetLastError());
     c->n_timed = i;
-    c->last_launches = i;
+    c->last_launches = launched;
     return MRA_OK;
 }
 
@@ -433,6 +443,29 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
         TALLOC(t.fbuf[p], double, f_sz[p]);
     }
     TALLOC(t.ws, T, (long)c->grid * t.ws_stride);
+    // covariance blocks of the prior levels: all of a level's blocks when they
+    // fit MRA_COV_BUF_MB (default 2048 MB), else the level runs in chunks of
+    // regions (a smaller buffer is tried when the first allocation fails)
+    t.cbuf = nullptr;
+    t.cbuf_elems = 0;
+    if (prior_part) {
+        long need = 0;
+        for (int m = 0; m <= M - 2; ++m) need = std::max(need, level_count(J, m) * (long)(m + 1) * rr);
+        long cap_mb = 2048;
+        if (const char* e = std::getenv("MRA_COV_BUF_MB")) cap_mb = std::max(1L, std::atol(e));
+        long elems = std::min(need, cap_mb * (1L << 20) / (long)sizeof(T));
+        const long floor_elems = std::min(need, (long)(M - 1) * rr * c->grid);  // one region per CTA slot
+        elems = std::max(elems, floor_elems);
+        for (;;) {
+            cudaError_t e2 = cudaSuccess;
+            t.cbuf = c->alloc<T>((size_t)elems, &e2);
+            if (!e2) break;
+            cudaGetLastError();
+            if (elems <= floor_elems) return fail(MRA_ERR_OOM, "device allocation failed: t.cbuf");
+            elems = std::max(floor_elems, elems / 4);
+        }
+        t.cbuf_elems = elems;
+    }
     TALLOC(t.wsd, double, (long)c->grid * t.wsd_stride);
     TALLOC(t.P, T, pred_part ? c->n_pred * (long)L * r : 1);
     TALLOC(t.Bt, T, pred_part ? c->n_pred * (long)L * r : 1);
@@ -807,6 +840,8 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
     if (c->graph_exec) {
         CU(cudaGraphLaunch(c->graph_exec, c->stream));
         c->stats.graph_replays++;
+        c->n_timed = c->graph_timed[0];
+        c->last_launches = c->graph_launches[0];
     } else {
         mra_status s = run_eval(c, false);
         if (s) return s;
@@ -823,6 +858,8 @@ mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     if (c->graph_pred_exec) {
         CU(cudaGraphLaunch(c->graph_pred_exec, c->stream));
         c->stats.graph_replays++;
+        c->n_timed = c->graph_timed[1];
+        c->last_launches = c->graph_launches[1];
     } else {
         mra_status s = run_eval(c, true);
         if (s) return s;
@@ -857,6 +894,8 @@ mra_status capture_one(mra_ctx* c, bool predict, cudaGraph_t* graph, cudaGraphEx
         return fail(MRA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
     }
     *graph = g;
+    c->graph_timed[predict ? 1 : 0] = c->n_timed;
+    c->graph_launches[predict ? 1 : 0] = c->last_launches;
     return MRA_OK;
 }
 
@@ -872,6 +911,22 @@ mra_status mra_capture_graph(mra_ctx* c) {
         mra_status s = capture_one(c, true, &c->graph_pred, &c->graph_pred_exec);
         if (s) return s;
     }
+    return MRA_OK;
+}
+
+mra_status mra_get_terms(mra_ctx* c, double* out, int32_t n_out) {
+    if (!c || !out) return fail(MRA_ERR_ARG, "NULL argument");
+    if (n_out < c->M) return fail(MRA_ERR_ARG, "mra_get_terms: n_out must be at least M");
+    CU(cudaStreamSynchronize(c->stream));
+    std::vector<double> dpost(c->n_int), dfin(level_count(c->J, c->M - 2));
+    CU(cudaMemcpy(dpost.data(), c->td.dpost, dpost.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(dfin.data(), c->td.dfin, dfin.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int m = 0; m < c->M; ++m) out[m] = 0.0;
+    for (int m = 0; m <= c->M - 2; ++m) {
+        const long s0 = level_start(c->J, m), cnt = level_count(c->J, m);
+        for (long q = 0; q < cnt; ++q) out[m] += dpost[s0 + q];
+    }
+    for (double v : dfin) out[c->M - 1] += v;
     return MRA_OK;
 }
 

@@ -253,6 +253,51 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
     return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
+// The same two quantities seeded by the single-precision approximations
+// (rcp.approx.ftz.f32 / rsqrt.approx.ftz.f32 of the argument rounded to FP32,
+// relative error near 2^-23) and refined by the same third-order Newton step,
+// whose cubic convergence takes the seed error below 2^-66: the result is within
+// an ulp or two of the FP64-seeded form.  The FP32 units issue these far faster
+// than the FP64 approximations; arguments outside [1e-30, 1e30], where the FP32
+// seed would underflow or overflow, take the FP64-seeded path.
+__device__ __forceinline__ double rcp_fast(double s) {
+    if (!(s > 1e-30 && s < 1e30)) return rcp_nr(s);
+    float yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(s)));
+    const double y = (double)yf;
+    const double e = fma(-s, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+}
+
+__device__ __forceinline__ double rsqrt_fast(double x) {
+    if (!(x > 1e-30 && x < 1e30)) return rsqrt_nr(x);
+    float yf;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(x)));
+    const double y = (double)yf;
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
+// One nonstationary straight-line entry from per-point quantities (see
+// fill_row_fast): row point (pc, ga, ca = sqrt(s1) b1 / scale^2 for PREF 1;
+// ssa, ba_h = b1 / scale^2 for PREF 0), column point (q, gq, ssbq = sqrt(s2) b2;
+// ssq, bq).
+template <int NU, int PREF>
+__device__ __forceinline__ double cov_fast_entry(double pc0, double pc1, double pc2, double ga, double ca,
+                                                 double ssa, double ba_h, double qx, double qy, double qz, double gq,
+                                                 double ssbq, double ssq, double bq) {
+    const double dx = qx - pc0, dy = qy - pc1, dz = qz - pc2;
+    const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+    const double w = rcp_fast(ga + gq);  // 2 scale^2 / (b1^2 + b2^2)
+    const double u = d2 * w;             // h^2
+    const double h = u > 1e-300 ? u * rsqrt_fast(u) : 0.0;
+    const double em = exp_neg(h);
+    const double m = NU == 3 ? (1.0 + h) * em : em;
+    if (PREF == 1) return (ca * ssbq) * w * m;
+    const double x = ba_h * bq * w;
+    return (ssa * ssq) * (x * sqrt(x)) * m;
+}
+
 // One row point against the staged column points q_begin, q_begin + q_step,
 // ... < q_end (straight-line distance, nonstationary): writes ob[(qoff + q) ld].
 // NU: 1 exponential, 3 Matern 3/2; PREF: 0 prefactor x^1.5, 1 prefactor x.
@@ -273,20 +318,9 @@ __device__ __noinline__ void fill_row_fast(const double* __restrict__ sx, const 
     const double ca = ssa * ba * ihs2, ba_h = ba * ihs2;
 #pragma unroll 4
     for (int q = q_begin; q < q_end; q += q_step) {
-        const double dx = sx[q] - pc0, dy = sy[q] - pc1, dz = sz[q] - pc2;
-        const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
-        const double w = rcp_nr(ga + sg[q]);  // 2 scale^2 / (b1^2 + b2^2)
-        const double u = d2 * w;              // h^2
-        const double h = u > 1e-300 ? u * rsqrt_nr(u) : 0.0;
-        const double em = exp_neg(h);
-        const double m = NU == 3 ? (1.0 + h) * em : em;
-        double v;
-        if (PREF == 1) {
-            v = (ca * ssb[q]) * w * m;
-        } else {
-            const double x = ba_h * sb[q] * w;
-            v = (ssa * ss[q]) * (x * sqrt(x)) * m;
-        }
+        const double v = cov_fast_entry<NU, PREF>(pc0, pc1, pc2, ga, ca, ssa, ba_h, sx[q], sy[q], sz[q], sg[q],
+                                                  PREF == 1 ? ssb[q] : 0.0, PREF == 1 ? 0.0 : ss[q],
+                                                  PREF == 1 ? 0.0 : sb[q]);
         ob[(long)(qoff + q) * ld] = (T)v;
     }
 }
@@ -303,11 +337,14 @@ __device__ __noinline__ void fill_row_fast(const double* __restrict__ sx, const 
 // fill_cov_blocks: nblk blocks of na rows each, block k from the row points
 // starting at a0[k], written to out + k * blk (same columns for every block);
 // `self` applies to block 0 only.
-template <typename T>
-__device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, const long* a0, int nblk, int na,
-                                             long b0, int nb, bool self, T* out, long ld, long blk, LaSmem<T>& sm) {
-    constexpr int CH = sizeof(T) == 8 ? 512 : 96;  // columns staged per chunk
-    double* sx = reinterpret_cast<double*>(&sm.A[0][0]);
+// fill_cov_staged: the same with the staging area given explicitly (7 CH
+// doubles) and CH columns staged per chunk; every entry is computed by the same
+// per-entry code whatever CH is.
+template <typename T, int CH>
+__device__ __noinline__ void fill_cov_staged(const Geom& g, const PointSet& P, const long* a0, int nblk, int na,
+                                             long b0, int nb, bool self, T* out, long ld, long blk,
+                                             double* stage) {
+    double* sx = stage;
     double* sy = sx + CH;
     double* sz = sy + CH;
     double* ss = sz + CH;
@@ -389,6 +426,14 @@ __device__ __noinline__ void fill_cov_blocks(const Geom& g, const PointSet& P, c
         }
     }
     __syncthreads();
+}
+
+template <typename T>
+__device__ inline void fill_cov_blocks(const Geom& g, const PointSet& P, const long* a0, int nblk, int na, long b0,
+                                       int nb, bool self, T* out, long ld, long blk, LaSmem<T>& sm) {
+    // the staging area is the tile buffers of sm: 7 CH doubles
+    fill_cov_staged<T, sizeof(T) == 8 ? 512 : 96>(g, P, a0, nblk, na, b0, nb, self, out, ld, blk,
+                                                   reinterpret_cast<double*>(&sm.A[0][0]));
 }
 
 template <typename T>

@@ -89,19 +89,180 @@ __global__ void k_fields(Geom g, FieldParams fp, const double* __restrict__ c0, 
 }
 
 // ---------------------------------------------------------------------------
+// a2/a3 for the prior: the covariance blocks of one level, in their own launch
+// ---------------------------------------------------------------------------
+// Regions loc0 .. loc0+nloc-1 (local indices) of level m: block j < m of region
+// i is C(Q_{a_j}, Q_i) (rows: the knots of ancestor a_j, columns: the region's
+// own knots; evaluate_nonstationary_cross_covariance, evaluate_covariance.cpp:
+// 155-234), block m is C(Q_i, Q_i) with sigma^2 + tau^2 on its diagonal
+// (:248-313).  Block j of the q-th region goes to out + (q (m+1) + j) r^2,
+// column-major with ld r.  One CTA per block at a time; with no barrier-bound
+// products beside it the launch keeps every SM full of independent entry
+// chains, which the per-region kernel, two CTAs per SM between its products,
+// cannot.
+constexpr int kCovThreads = 256;
+constexpr int kCovChunk = 64;  // column points staged per chunk (7 x 64 doubles of shared memory)
+
+// The straight-line nonstationary FP64 block: one row point per thread with its
+// parameters in registers, the column points staged in chunks, entries of
+// cov_fast_entry (the same arithmetic as fill_row_fast).
+template <typename T, int NU, int PREF>
+__device__ __forceinline__ void cov_block_fast(const PointSet& P, long a0, int nr, long b0, int nc, bool self,
+                                               T* __restrict__ out, long ld, double ih2, double ihs2,
+                                               double* stage) {
+    double* sx = stage;
+    double* sy = sx + kCovChunk;
+    double* sz = sy + kCovChunk;
+    double* sg = sz + kCovChunk;
+    double* s4 = sg + kCovChunk;  // sqrt(s2) b (PREF 1) or sqrt(s2) (PREF 0)
+    double* s5 = s4 + kCovChunk;  // b (PREF 0)
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int rows = nr < nt ? nr : nt;
+    const int cols = nt / rows;
+    const bool worker = tid < rows * cols;
+    const int tr = tid % rows, tc = tid / rows;
+    for (int q0 = 0; q0 < nc; q0 += kCovChunk) {
+        const int qn = nc - q0 < kCovChunk ? nc - q0 : kCovChunk;
+        __syncthreads();
+        for (int e = tid; e < qn; e += nt) {
+            const long ib = b0 + q0 + e;
+            const double bb = P.beta[ib], ssq = sqrt(P.s2[ib]);
+            sx[e] = P.c0[ib];
+            sy[e] = P.c1[ib];
+            sz[e] = P.c2[ib];
+            sg[e] = bb * bb * ih2;
+            s4[e] = PREF == 1 ? ssq * bb : ssq;
+            s5[e] = bb;
+        }
+        __syncthreads();
+        if (!worker) continue;
+        for (int t = tr; t < nr; t += rows) {
+            const long ia = a0 + t;
+            const double pc0 = P.c0[ia], pc1 = P.c1[ia], pc2 = P.c2[ia], sa = P.s2[ia], ba = P.beta[ia];
+            const double ssa = sqrt(sa), ga = ba * ba * ih2, ca = ssa * ba * ihs2, ba_h = ba * ihs2;
+            const double diag = self ? sa + P.t2[ia] : 0.0;
+            T* ob = out + t;
+#pragma unroll 4
+            for (int q = tc; q < qn; q += cols) {
+                const int qq = q0 + q;
+                double v = cov_fast_entry<NU, PREF>(pc0, pc1, pc2, ga, ca, ssa, ba_h, sx[q], sy[q], sz[q], sg[q],
+                                                    PREF == 1 ? s4[q] : 0.0, PREF == 1 ? 0.0 : s4[q],
+                                                    PREF == 1 ? 0.0 : s5[q]);
+                if (self && t == qq) v = diag;  // sigma^2 + tau^2 (evaluate_covariance.cpp:103,307)
+                ob[(long)qq * ld] = (T)v;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Block out[t + q ld] = C(A_{a0+t}, B_{b0+q}), t < nr, q < nc (with the
+// sigma^2 + tau^2 diagonal when `self`), by the whole CTA.  KIND (cov_kind on the
+// host): 1..4 the straight-line nonstationary FP64 forms (Matern 3/2 or 1/2 x
+// prefactor exponent 1 or 3/2), 0 every other model.
+template <typename T, int KIND>
+__device__ __forceinline__ void cov_block(const Geom& g, const PointSet& P, long a0, int nr, long b0, int nc, bool self,
+                                          T* out, long ld, double* stage) {
+    if constexpr (KIND == 0) {
+        fill_cov_staged<T, kCovChunk>(g, P, &a0, 1, nr, b0, nc, self, out, ld, 0, stage);
+    } else {
+        const double hs = g.dist_scale * (KIND <= 2 ? 1.7320508075688772 : 1.0);
+        const double ihs2 = 1.0 / (hs * hs), ih2 = 0.5 * ihs2;
+        constexpr int NU = KIND <= 2 ? 3 : 1, PREF = (KIND & 1) ? 1 : 0;
+        cov_block_fast<T, NU, PREF>(P, a0, nr, b0, nc, self, out, ld, ih2, ihs2, stage);
+    }
+}
+
+inline int cov_kind(const Geom& g, bool fp64) {
+    if (!(fp64 && g.nonstat && g.distance != 1 && g.pref_kind != 2)) return 0;
+    return g.nu_x2 == 3 ? (g.pref_kind == 1 ? 1 : 2) : (g.pref_kind == 1 ? 3 : 4);
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kCovThreads, 4) k_cov_level(Geom g, DevTree<T> t, int m, long loc0, long nloc,
+                                                               T* __restrict__ out) {
+    __shared__ double stage[7 * kCovChunk];
+    const int r = t.r;
+    const long rr = (long)r * r;
+    const long s0 = level_start(t.J, m);
+    const long nblocks = nloc * (m + 1);
+    for (long b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const long q = b / (m + 1);
+        const int j = (int)(b - q * (m + 1));
+        const long i = s0 + loc0 + q;
+        long a = i;  // the ancestor of level j (the region itself for j == m)
+        for (int l = m; l > j; --l) a = (a - 1) / t.J;
+        cov_block<T, KIND>(g, t.pts, a * r, r, i * r, r, j == m, out + b * rr, r, stage);
+    }
+}
+
+// The finest level's blocks against the ancestors, in their own launch before
+// k_finest_group: for every level M-2 region p (a sibling group: its finest
+// children's observations S_p are contiguous) and every level j = 0..M-2, the
+// block C(Q_{a_j}, S_p) (a_{M-2} = p) into the rows of B^ (obs-major, ld L r),
+// which the finest kernel then conditions in place
+// (...-loop-regions-at-finest-level-in-prior.cpp:116-160).
+template <typename T, int KIND>
+__global__ void __launch_bounds__(kCovThreads, 4) k_cov_finest(Geom g, DevTree<T> t) {
+    __shared__ double stage[7 * kCovChunk];
+    const int r = t.r, L = t.L, m = t.M - 2;
+    const long Lr = (long)L * r;
+    const long s2 = level_start(t.J, m), cnt2 = level_count(t.J, m);
+    const long nblocks = cnt2 * L;
+    for (long b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const long ploc = b / L;
+        const int j = (int)(b - ploc * L);
+        const long lo = t.obs_off[t.child_lo[ploc]];
+        const int np = (int)(t.obs_off[t.child_hi[ploc]] - lo);
+        if (np == 0) continue;
+        long a = s2 + ploc;
+        for (int l = m; l > j; --l) a = (a - 1) / t.J;
+        cov_block<T, KIND>(g, t.pts, a * r, r, t.obs0 + lo, np, false, t.Bhat + lo * Lr + (long)j * r, Lr, stage);
+    }
+}
+
+// Host-side dispatch of the covariance-block launches on the model's form.
+template <typename T>
+void launch_cov_level(const Geom& g, const DevTree<T>& t, int m, long loc0, long n, unsigned grid, cudaStream_t st) {
+    switch (cov_kind(g, sizeof(T) == 8)) {
+        case 1: k_cov_level<T, 1><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
+        case 2: k_cov_level<T, 2><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
+        case 3: k_cov_level<T, 3><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
+        case 4: k_cov_level<T, 4><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
+        default: k_cov_level<T, 0><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
+    }
+}
+template <typename T>
+void launch_cov_finest(const Geom& g, const DevTree<T>& t, unsigned grid, cudaStream_t st) {
+    switch (cov_kind(g, sizeof(T) == 8)) {
+        case 1: k_cov_finest<T, 1><<<grid, kCovThreads, 0, st>>>(g, t); break;
+        case 2: k_cov_finest<T, 2><<<grid, kCovThreads, 0, st>>>(g, t); break;
+        case 3: k_cov_finest<T, 3><<<grid, kCovThreads, 0, st>>>(g, t); break;
+        case 4: k_cov_finest<T, 4><<<grid, kCovThreads, 0, st>>>(g, t); break;
+        default: k_cov_finest<T, 0><<<grid, kCovThreads, 0, st>>>(g, t); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // a5/a6: prior, one level of interior regions
 // ---------------------------------------------------------------------------
 // One CTA per region.  The inverse L_a^{-1} of every prior factor is formed
 // once, right after its Cholesky, so that the m triangular solves of each
-// descendant become tensor-pipe products.
+// descendant become tensor-pipe products.  The covariance blocks come from
+// k_cov_level (C: the q-th region's m+1 blocks at C + q (m+1) r^2); each
+// conditioning product takes its block as the added term, so nothing is
+// copied: V_j = C_j - U_{a_j}^T U_{i,0..j-1}, U_{i,j} = L_{a_j}^{-1} V_j and
+// K_i = C_i - U_i^T U_i straight into the factor's storage.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> t, int m) {
+__global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> t, int m, long loc0, long nloc,
+                                                            const T* __restrict__ C) {
     LaSmem<T>& sm = la_smem<T>();
     const int r = t.r;
     const long rr = (long)r * r;
-    const long s0 = level_start(t.J, m), cnt = level_count(t.J, m);
+    const long s0 = level_start(t.J, m);
     const long mr = (long)m * r;
-    for (long loc = blockIdx.x; loc < cnt; loc += gridDim.x) {
+    for (long q = blockIdx.x; q < nloc; q += gridDim.x) {
+        const long loc = loc0 + q;
         const long i = s0 + loc;
         long anc[kMaxLevels];
         {
@@ -111,24 +272,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
                 anc[a] = c;
             }
         }
+        const T* Cq = C + q * (long)(m + 1) * rr;
         T* Ui = t.U + t.u_off[m] + loc * mr * r;  // (m r) x r, ld = m r
-        // one r x r scratch per CTA (stays in L2; a scratch for all m ancestors at
-        // once doubled the DRAM traffic of the launch at no gain in time)
+        // one r x r scratch per CTA (stays in L2)
         T* V = t.ws + blockIdx.x * t.ws_stride;
         for (int j = 0; j < m; ++j) {
             const long a = anc[j];
-            fill_cov<T>(g, t.pts, a * r, r, i * r, r, false, V, r, sm);
+            const T* Cj = Cq + j * rr;
+            const T* Vj = Cj;  // level 0 has nothing to condition on
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm);
+                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm, Cj, r);
+                Vj = V;
             }
             // U_{i,j} = L_a^{-1} V as a product with the stored inverse
-            gemm<T, false, false>(r, r, r, (T)1, t.Pinv + a * rr, r, V, r, (T)0, Ui + (long)j * r, mr, sm);
+            gemm<T, false, false>(r, r, r, (T)1, t.Pinv + a * rr, r, Vj, r, (T)0, Ui + (long)j * r, mr, sm);
         }
         T* Li = t.Lprior + i * rr;
-        fill_cov<T>(g, t.pts, i * r, r, i * r, r, true, Li, r, sm);
-        __syncthreads();
-        if (m > 0) gemm<T, true, false>(r, r, (int)mr, (T)-1, Ui, mr, Ui, mr, (T)1, Li, r, sm);
+        // K_i = C_i - U_i^T U_i (for m == 0 a product with K = 0: the copy of C_i)
+        gemm<T, true, false>(r, r, (int)mr, (T)-1, Ui, mr, Ui, mr, (T)1, Li, r, sm, Cq + (long)m * rr, r);
         double ld = 0.0;
         int info = potrf_lower<T>(r, Li, r, sm, &ld, t.Pinv + i * rr, r);
         if (threadIdx.x == 0) {
@@ -479,12 +641,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
         const long ulo = t.sub_lo[ui];
         const int nu = (int)(t.sub_hi[ui] - ulo);
         if (m > 0 && nu > 0) {
-            // C(Q_{a_j}, S) of levels 0..M-3 for all observations of the unit, into B^
+            // B^ holds C(Q_{a_j}, S) of every level (k_cov_finest); conditioned in place
             T* Uf = t.Ufin + ulo * Lr;  // (L r) x nu, ld = L r
             T* Bh = t.Bhat + ulo * Lr;
-            long aoff[kMaxLevels];
-            for (int j = 0; j < m; ++j) aoff[j] = anc[j] * r;
-            fill_cov_blocks<T>(g, t.pts, aoff, m, r, t.obs0 + ulo, nu, false, Bh, Lr, r, sm);
             for (int j = 0; j < m; ++j) {
                 const long a = anc[j];
                 T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
@@ -504,9 +663,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
             if (np > 0) {
                 // level M-2: the group's own parent p
                 T* Uf = t.Ufin + lo * Lr;
-                T* V = t.Bhat + lo * Lr + (long)m * r;
-                const long ap = p * r;
-                fill_cov_blocks<T>(g, t.pts, &ap, 1, r, t.obs0 + lo, np, false, V, Lr, 0, sm);
+                T* V = t.Bhat + lo * Lr + (long)m * r;  // C(Q_p, S) from k_cov_finest
                 if (m > 0) {
                     const T* Ua = t.U + t.u_off[m] + ploc * (long)m * rr;
                     gemm<T, true, false>(r, np, m * r, (T)-1, Ua, (long)m * r, Uf, Lr, (T)1, V, Lr, sm);
@@ -833,14 +990,31 @@ void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const
     k_fields<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, fp, c0, c1, c2, n, s2, beta, t2);
 }
 template <typename T>
-void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st) {
-    long cnt = level_count(t.J, m);
-    k_prior_level<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, m);
+int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st) {
+    const long cnt = level_count(t.J, m);
+    const long per_region = (long)(m + 1) * t.r * t.r;
+    long per = t.cbuf_elems / per_region;  // regions whose blocks fit the buffer at once
+    if (per < 1) per = 1;
+    int launches = 0;
+    for (long loc0 = 0; loc0 < cnt; loc0 += per) {
+        const long n = cnt - loc0 < per ? cnt - loc0 : per;
+        const long nb = n * (m + 1);
+        const long cov_grid = (long)grid * 16;  // 16 per region-kernel slot: 32 CTAs per SM
+        launch_cov_level<T>(g, t, m, loc0, n, (unsigned)(nb < cov_grid ? nb : cov_grid), st);
+        k_prior_level<T><<<(unsigned)(n < grid ? n : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, m, loc0, n,
+                                                                                                t.cbuf);
+        launches += 2;
+    }
+    return launches;
 }
 template <typename T>
-void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
+int launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
+    const long nb = level_count(t.J, t.M - 2) * t.L;
+    const long cov_grid = (long)grid * 16;
+    launch_cov_finest<T>(g, t, (unsigned)(nb < cov_grid ? nb : cov_grid), st);
     long cnt = t.n_fin_items;
     k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, keep ? 1 : 0);
+    return 2;
 }
 template <typename T>
 void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st) {
@@ -901,8 +1075,8 @@ cudaError_t prepare_kernels() {
 }
 
 #define MRA_INSTANTIATE(T)                                                                                   \
-    template void launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t);            \
-    template void launch_finest_group<T>(const Geom&, const DevTree<T>&, int, bool, cudaStream_t);          \
+    template int launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t);             \
+    template int launch_finest_group<T>(const Geom&, const DevTree<T>&, int, bool, cudaStream_t);           \
     template void launch_posterior_level<T>(const Geom&, const DevTree<T>&, int, int, bool, cudaStream_t);  \
     template void launch_predict<T>(const Geom&, const DevTree<T>&, int, cudaStream_t);                     \
     template void launch_reduce<T>(const DevTree<T>&, double*, cudaStream_t);                               \

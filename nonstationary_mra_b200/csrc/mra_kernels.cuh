@@ -57,6 +57,8 @@ struct DevTree {
     double* wout[2];           // dense w~ of one level's dense regions (by dslot)
     T* Fbuf[2];                // factored F of one level: [n_obs][m r]
     double* fbuf[2];           // factored f of one level: [n_obs]
+    T* cbuf;                   // covariance blocks of a chunk of one prior level's regions
+    long cbuf_elems;           // its size in elements (a multiple of nothing in particular)
     T* ws;                     // per-CTA workspace (T)
     long ws_stride;
     double* wsd;               // per-CTA workspace (FP64)
@@ -114,10 +116,14 @@ cudaError_t set_gemm_tiles(const int nw[3]);
 
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
+// Covariance-block launches and region launches of one prior level, in chunks
+// of regions whose blocks fit t.cbuf; returns the number of kernels launched.
 template <typename T>
-void launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st);
+int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st);
+// The finest level's covariance blocks against the ancestors, then the finest
+// groups; returns the number of kernels launched (2).
 template <typename T>
-void launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st);
+int launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st);
 template <typename T>
 void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st);
 template <typename T>

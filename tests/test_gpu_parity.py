@@ -189,6 +189,15 @@ def test_prediction_graph_replay():
     ctx.close()
 
 
+def test_terms_sum_to_d():
+    st, md = random_case(14, 4, 5, 16, 3000, 10, clustered=True)
+    ctx, (d, _) = run_loglik(st, md)
+    t = ctx.terms()
+    assert t.shape == (st.M,)
+    assert abs(t.sum() - d) <= 1e-12 * max(1.0, abs(d))
+    ctx.close()
+
+
 def test_autotune_keeps_results_bitwise():
     st, md = random_case(12, 4, 4, 16, 1500, 10, clustered=True)
     ctx, (d0, _) = run_loglik(st, md)
