@@ -534,18 +534,26 @@ def predict_arm(args):
 
 def mixed_report_arm(args):
     """Attribution of the mixed path's error and time, stage by stage, on the
-    device: both precisions evaluate the same tree and values; for every launch
-    its CUDA-event time, and for every part of d (posterior terms of each interior
-    level; finest-level terms with the level M-2 posterior) the mixed path's
-    difference from FP64.  Repeated with y = 0, where d is the log-determinants
-    alone, to separate them from the quadratic forms."""
+    device.  Every variant evaluates the same tree and values: FP64, the mixed
+    path (prior levels and finest level in FP32, posterior FP64), and the mixed
+    path with only the prior levels or only the finest level in FP32
+    (MRA_MIXED_FP32).  For each: the device time of every launch and the error of
+    d and of the log-likelihood against FP64, with the observed values and with
+    y = 0, where d is the log-determinants alone (separating them from the
+    quadratic forms); and the error of every part of d (mra_get_terms)."""
     from nonstationary_mra_b200 import api, synth
     cfg = synth.CONFIGS[args.config]
     xy, pred, theta, md, st = make_problem(cfg)
     out = {"metric": "mixed-path attribution", "workload": workload_name(cfg), "M": cfg.M}
+    variants = [("fp64", "fp64", None), ("mixed", "mixed", "prior,finest"), ("mixed-prior-only", "mixed", "prior"),
+                ("mixed-finest-only", "mixed", "finest")]
     runs = {}
     y = None
-    for prec in ("fp64", "mixed"):
+    for name, prec, stages in variants:
+        if stages is None:
+            os.environ.pop("MRA_MIXED_FP32", None)
+        else:
+            os.environ["MRA_MIXED_FP32"] = stages
         ctx = api.Context(st, md, precision=prec)
         if y is None:
             y = draw_values(ctx, st, cfg.seed + 7)
@@ -558,23 +566,27 @@ def mixed_report_arm(args):
             d, ll = ctx.loglik()
             stats = ctx.stats()
             res[label] = {"d": d, "loglik": ll, "terms": ctx.terms().tolist(),
-                          "launches": [(l["kernel"], l["level"], l["ms"]) for l in stats["launches"]],
-                          "ms_total": stats["ms_total"]}
+                          "launches": [(l["kernel"], l["level"], round(l["ms"], 3)) for l in stats["launches"]],
+                          "ms_total": stats["ms_total"],
+                          "stage_ms": {k: stats[k] for k in ("ms_prior", "ms_finest", "ms_posterior")}}
         ctx.close()
-        runs[prec] = res
-    for label in ("y", "y0"):
-        a, b = runs["fp64"][label], runs["mixed"][label]
-        parts = []
-        for m in range(cfg.M):
-            name = f"posterior terms, level {m}" if m < cfg.M - 1 else "finest terms + level M-2 posterior"
-            parts.append({"part": name, "fp64": a["terms"][m], "mixed_minus_fp64": b["terms"][m] - a["terms"][m]})
-        out[label] = {"d_fp64": a["d"], "d_mixed": b["d"], "d_rel_err": abs(b["d"] - a["d"]) / abs(a["d"]),
-                      "loglik_fp64": a["loglik"], "loglik_mixed": b["loglik"],
-                      "loglik_rel_err": abs(b["loglik"] - a["loglik"]) / abs(a["loglik"]), "parts": parts}
-    la = runs["fp64"]["y"]["launches"]
-    lb = runs["mixed"]["y"]["launches"]
-    out["launch_ms"] = {"fp64": la, "mixed": lb, "fp64_total": runs["fp64"]["y"]["ms_total"],
-                        "mixed_total": runs["mixed"]["y"]["ms_total"]}
+        runs[name] = res
+    os.environ.pop("MRA_MIXED_FP32", None)
+    ref = runs["fp64"]
+    for name, _, _ in variants[1:]:
+        v = {}
+        for label in ("y", "y0"):
+            a, b = ref[label], runs[name][label]
+            v[label] = {"d_minus_fp64": b["d"] - a["d"], "d_rel_err": abs(b["d"] - a["d"]) / abs(a["d"]),
+                        "loglik_rel_err": abs(b["loglik"] - a["loglik"]) / abs(a["loglik"]),
+                        "parts_minus_fp64": [bt - at for at, bt in zip(a["terms"], b["terms"])]}
+        v["ms_total"] = runs[name]["y"]["ms_total"]
+        v["stage_ms"] = runs[name]["y"]["stage_ms"]
+        v["launches"] = runs[name]["y"]["launches"]
+        out[name] = v
+    out["fp64"] = {"d": ref["y"]["d"], "loglik": ref["y"]["loglik"], "d_y0": ref["y0"]["d"],
+                   "ms_total": ref["y"]["ms_total"], "stage_ms": ref["y"]["stage_ms"], "launches": ref["y"]["launches"],
+                   "parts": ref["y"]["terms"]}
     print(json.dumps(out))
 
 

@@ -86,6 +86,9 @@ struct mra_ctx {
     mra_stats stats{};
     int last_launches = 0;
     bool have_pred = false;
+    // mixed path stages kept in FP32 (a diagnostic switch, MRA_MIXED_FP32):
+    // the prior levels and the finest level; the posterior is always FP64
+    bool mixed_prior32 = true, mixed_finest32 = true;
 
     void* alloc_bytes(size_t bytes_, cudaError_t* err) {
         DevBuf b;
@@ -276,18 +279,36 @@ mra_status run_eval(mra_ctx* c, bool predict) {
                 launched += 1;
                 break;
             case MRA_KERNEL_PRIOR_LEVEL:
-                if (mixed) launched += launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
+                if (mixed && c->mixed_prior32) launched += launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
                 else launched += launch_prior_level<double>(c->geom, td, l.level, c->grid, st);
                 break;
             case MRA_KERNEL_FINEST:
-                if (mixed) launched += launch_finest_group<float>(c->geom, tf, c->grid, predict, st);
+                if (mixed && c->mixed_prior32 != c->mixed_finest32) {
+                    // the finest level runs in the other precision: its ancestors' factors follow it
+                    if (c->mixed_prior32) {
+                        launch_convert<float, double>(tf.U, td.U, c->u_total, st);
+                        launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
+                        launch_convert<float, double>(tf.Pinv, td.Pinv, c->n_int * rr, st);
+                    } else {
+                        launch_convert<double, float>(td.U, tf.U, c->u_total, st);
+                        launch_convert<double, float>(td.Lprior, tf.Lprior, c->n_int * rr, st);
+                        launch_convert<double, float>(td.Pinv, tf.Pinv, c->n_int * rr, st);
+                    }
+                    launched += 3;
+                }
+                if (mixed && c->mixed_finest32) launched += launch_finest_group<float>(c->geom, tf, c->grid, predict, st);
                 else launched += launch_finest_group<double>(c->geom, td, c->grid, predict, st);
                 break;
             case MRA_KERNEL_CONVERT:
-                launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
-                launch_convert<float, double>(tf.Pinv, td.Pinv, c->n_int * rr, st);
-                launch_convert<float, double>(tf.Bhat, td.Bhat, c->n_obs * (long)c->L * c->r, st);
-                launched += 3;
+                if (c->mixed_prior32 && c->mixed_finest32) {
+                    launch_convert<float, double>(tf.Lprior, td.Lprior, c->n_int * rr, st);
+                    launch_convert<float, double>(tf.Pinv, td.Pinv, c->n_int * rr, st);
+                    launched += 2;
+                }
+                if (c->mixed_finest32) {
+                    launch_convert<float, double>(tf.Bhat, td.Bhat, c->n_obs * (long)c->L * c->r, st);
+                    launched += 1;
+                }
                 break;
             case MRA_KERNEL_POSTERIOR_LEVEL:
                 launch_posterior_level<double>(c->geom, td, l.level, c->grid, predict, st);
@@ -763,8 +784,15 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     c->u_total = u_total;
     mra_status st;
     if (precision == MRA_PRECISION_MIXED) {
+        if (const char* e = std::getenv("MRA_MIXED_FP32")) {
+            const std::string v(e);
+            c->mixed_prior32 = v.find("prior") != std::string::npos;
+            c->mixed_finest32 = v.find("finest") != std::string::npos;
+        }
+        const bool both = c->mixed_prior32 && c->mixed_finest32;
         st = setup_tree<float>(c, c->tf32, h, pts, y, idx, u_total, sh, true, false, c->have_pred);
-        if (!st) st = setup_tree<double>(c, c->td, h, pts, y, idx, u_total, sh, false, true, false);
+        if (!st) st = setup_tree<double>(c, c->td, h, pts, y, idx, u_total, sh, !both, true, false);
+        c->td.fuse_post = 0;  // the plan runs the level M-2 posterior on its own
     } else {
         st = setup_tree<double>(c, c->td, h, pts, y, idx, u_total, sh, true, true, c->have_pred);
     }
@@ -855,6 +883,8 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
 mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     if (!c) return fail(MRA_ERR_ARG, "NULL context");
     if (!c->have_pred) return fail(MRA_ERR_STATE, "the structure has no prediction locations");
+    if (!(c->mixed_prior32 && c->mixed_finest32))
+        return fail(MRA_ERR_STATE, "prediction needs the mixed path with both FP32 stages (MRA_MIXED_FP32)");
     if (c->graph_pred_exec) {
         CU(cudaGraphLaunch(c->graph_pred_exec, c->stream));
         c->stats.graph_replays++;
@@ -986,6 +1016,8 @@ mra_status mra_autotune(mra_ctx* c, int32_t evals, int32_t* choice_out, double* 
 
 mra_status mra_sample_prior(mra_ctx* c, const double* z_int, const double* z_obs, double* y_out) {
     if (!c || !z_int || (!z_obs && c->n_obs) || (!y_out && c->n_obs)) return fail(MRA_ERR_ARG, "NULL argument");
+    if (!(c->mixed_prior32 && c->mixed_finest32))
+        return fail(MRA_ERR_STATE, "sampling needs the mixed path with both FP32 stages (MRA_MIXED_FP32)");
     // the prior factors (U of the finest level, L_Sigma) come from one evaluation
     mra_status s = run_eval(c, false);
     if (s) return s;

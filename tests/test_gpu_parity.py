@@ -272,3 +272,18 @@ def test_mixed_golden_predict_error_report(case_dir):
     print(f"mixed prediction err {os.path.basename(case_dir)}: mean {em:.3e} var {ev:.3e}")
     assert em <= 1e-4 and ev <= 1e-4
     ctx.close()
+
+
+@pytest.mark.parametrize("stages", ["", "prior", "finest"])
+def test_mixed_stage_switch(stages, monkeypatch):
+    """The mixed path's per-stage precision switch (MRA_MIXED_FP32): with neither
+    stage in FP32 it runs the mixed schedule in FP64 and matches the oracle to the
+    FP64 tolerance; with one stage in FP32 it stays within the mixed tolerance."""
+    st, md = random_case(15, 4, 4, 16, 2000, 10, clustered=True)
+    ost, omd = to_oracle(st, md)
+    d_ref, ll_ref = oracle.loglik(ost, omd)
+    monkeypatch.setenv("MRA_MIXED_FP32", stages)
+    ctx, (d, ll) = run_loglik(st, md, precision="mixed")
+    ctx.close()
+    tol = LL_RTOL if stages == "" else MIXED_LL_RTOL
+    assert abs(ll - ll_ref) <= tol * abs(ll_ref), (stages, ll, ll_ref)
