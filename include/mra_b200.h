@@ -253,6 +253,43 @@ mra_status mra_timer_stop(mra_ctx* ctx, double* ms);
 mra_status mra_eval_covariance_static(const mra_model* m, const mra_theta* theta, const double* p1_dev, uint64_t n1,
                                       const double* p2_dev, uint64_t n2, int32_t self, double* out_dev, void* stream);
 
+/* Sub-tree sharding: one log-likelihood over several GPUs, one process (and
+ * context, on the same structure) per GPU.  The tree splits at level s into J^s
+ * independent sub-trees, as the reference's MPI build splits its regions among
+ * ranks (src/class_partition.cpp:1188-1280) and sums the children's
+ * contributions on the parent's rank (src/class_approximation.cpp:186-264).
+ *
+ *   mra_shard_set(ctx, s, owned)      owned[q] != 0 for the level-s regions q
+ *                                     (local index 0..J^s-1) this rank computes;
+ *                                     1 <= s <= M-3, FP64 path; owned = NULL
+ *                                     returns the context to whole evaluations
+ *   mra_shard_loglik_subtrees(ctx)    prior of levels < s (every rank), and the
+ *                                     prior, finest level and posterior of levels
+ *                                     >= s of the owned sub-trees
+ *   mra_shard_record_size/export      the owned region q's record: its output to
+ *                                     its parent (the reference's A~ and w~, or the
+ *                                     factored F, f) and the log-likelihood terms of
+ *                                     its sub-tree, n_doubles doubles of host memory
+ *   mra_shard_import                  on the rank that finishes: the records of the
+ *                                     regions it does not own
+ *   mra_shard_loglik_top(ctx, &d, &l) posterior of levels < s and the sum, on the
+ *                                     finishing rank after every import: bitwise the
+ *                                     whole evaluation's d (every term is computed by
+ *                                     the same kernel code and summed in the same order)
+ *
+ * Record layout (doubles): [kind (0 dense, 1 factored), rows] then the dense
+ * slices (s(s+1)/2 r x r, then s r) or the factored rows (rows x s r, then rows),
+ * then the posterior terms of the sub-tree's regions level by level (J^(m-s) for
+ * m = s..M-2), then the finest-level terms of its J^(M-2-s) sibling groups.
+ * While a context is sharded, mra_loglik, mra_predict, mra_sample_prior and
+ * mra_capture_graph return MRA_ERR_STATE. */
+mra_status mra_shard_set(mra_ctx* ctx, int32_t split_level, const uint8_t* owned);
+mra_status mra_shard_loglik_subtrees(mra_ctx* ctx);
+mra_status mra_shard_record_size(const mra_ctx* ctx, uint64_t region, uint64_t* n_doubles);
+mra_status mra_shard_export(mra_ctx* ctx, uint64_t region, double* record, uint64_t n_doubles);
+mra_status mra_shard_import(mra_ctx* ctx, uint64_t region, const double* record, uint64_t n_doubles);
+mra_status mra_shard_loglik_top(mra_ctx* ctx, double* d_out, double* loglik_out);
+
 /* Text of the last error on this thread. */
 const char* mra_last_error(void);
 

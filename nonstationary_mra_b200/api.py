@@ -159,6 +159,36 @@ class Context:
                             "ms": s.timed_ms[i], "flop": s.timed_flop[i]} for i in range(n)]
         return out
 
+    # ---- sub-tree sharding (include/mra_b200.h: mra_shard_*) ----
+    def shard_set(self, split_level: int, owned) -> None:
+        """Restrict evaluations to the level-`split_level` sub-trees with owned[q]
+        true; owned = None returns the context to whole evaluations."""
+        if owned is None:
+            check(self._lib.mra_shard_set(self._h, 0, None), "mra_shard_set")
+            return
+        o = np.ascontiguousarray(np.asarray(owned, dtype=np.uint8))
+        check(self._lib.mra_shard_set(self._h, int(split_level), o.ctypes.data_as(C.POINTER(C.c_uint8))),
+              "mra_shard_set")
+
+    def shard_subtrees(self) -> None:
+        check(self._lib.mra_shard_loglik_subtrees(self._h), "mra_shard_loglik_subtrees")
+
+    def shard_export(self, region: int) -> np.ndarray:
+        n = C.c_uint64()
+        check(self._lib.mra_shard_record_size(self._h, int(region), C.byref(n)), "mra_shard_record_size")
+        rec = np.empty(n.value)
+        check(self._lib.mra_shard_export(self._h, int(region), f64p(rec), n.value), "mra_shard_export")
+        return rec
+
+    def shard_import(self, region: int, record: np.ndarray) -> None:
+        rec = _c(record, np.float64)
+        check(self._lib.mra_shard_import(self._h, int(region), f64p(rec), rec.shape[0]), "mra_shard_import")
+
+    def shard_top(self):
+        d, ll = C.c_double(), C.c_double()
+        check(self._lib.mra_shard_loglik_top(self._h, C.byref(d), C.byref(ll)), "mra_shard_loglik_top")
+        return d.value, ll.value
+
     def terms(self) -> np.ndarray:
         """Parts of d from the last evaluation: [m] = level-m posterior terms for
         m < M-1, [M-1] = finest-level plus level M-2 terms (mra_get_terms)."""

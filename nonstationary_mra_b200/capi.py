@@ -85,6 +85,12 @@ SIGNATURES = [
     ("mra_capture_graph", C.c_int, [C.c_void_p]),
     ("mra_get_stats", C.c_int, [C.c_void_p, C.POINTER(mra_stats)]),
     ("mra_get_terms", C.c_int, [C.c_void_p, _p_f64, C.c_int32]),
+    ("mra_shard_set", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint8)]),
+    ("mra_shard_loglik_subtrees", C.c_int, [C.c_void_p]),
+    ("mra_shard_record_size", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("mra_shard_export", C.c_int, [C.c_void_p, C.c_uint64, _p_f64, C.c_uint64]),
+    ("mra_shard_import", C.c_int, [C.c_void_p, C.c_uint64, _p_f64, C.c_uint64]),
+    ("mra_shard_loglik_top", C.c_int, [C.c_void_p, _p_f64, _p_f64]),
     ("mra_sample_prior", C.c_int, [C.c_void_p, _p_f64, _p_f64, _p_f64]),
     ("mra_eval_covariance", C.c_int, [C.POINTER(mra_model), C.POINTER(mra_theta), _p_f64, C.c_uint64, _p_f64,
                                       C.c_uint64, C.c_int32, _p_f64]),

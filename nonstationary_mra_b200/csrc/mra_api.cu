@@ -67,6 +67,15 @@ struct mra_ctx {
     std::vector<Launch> plan;  // launches of one log-likelihood, in order
     double flop_predict_launch = 0;
     int n_timed = 0;
+    std::vector<int> timed_plan;  // plan index of each timed launch of the last evaluation (-1: prediction)
+    // sub-tree sharding: split level (0 = off), the device mask of computed
+    // regions, and the evaluation phase (0 whole, 1 own sub-trees, 2 top levels)
+    int shard_split = 0;
+    int8_t* d_active = nullptr;
+    int eval_phase = 0;
+    std::vector<int8_t> h_factored;          // [n_int] posterior output kept as F, f
+    std::vector<int64_t> h_sub_lo, h_sub_hi;  // [n_int] observation range of each sub-tree
+    std::vector<int64_t> h_dslot;            // [n_int] slot among the level's dense regions
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     // prior -> posterior (predictive factors kept) -> prediction, when the
@@ -270,7 +279,16 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     const long np_all = c->n_int * c->r + c->n_obs + c->n_pred;
     const long rr = (long)c->r * c->r;
     int i = 0, launched = 0;
-    for (const auto& l : c->plan) {
+    c->timed_plan.clear();
+    for (size_t pi = 0; pi < c->plan.size(); ++pi) {
+        const auto& l = c->plan[pi];
+        if (c->eval_phase != 0) {
+            // phase 1: everything of the own sub-trees (levels >= split); phase 2: the levels above + the sum
+            const bool top = (l.kind == MRA_KERNEL_POSTERIOR_LEVEL && l.level < c->shard_split) ||
+                             l.kind == MRA_KERNEL_REDUCE;
+            if (top != (c->eval_phase == 2)) continue;
+        }
+        c->timed_plan.push_back((int)pi);
         CU(record(c->tev[2 * i], st, capturing));
         switch (l.kind) {
             case MRA_KERNEL_FIELDS:
@@ -323,6 +341,7 @@ mra_status run_eval(mra_ctx* c, bool predict) {
         ++i;
     }
     if (predict) {
+        c->timed_plan.push_back(-1);
         CU(record(c->tev[2 * i], st, capturing));
         if (mixed) {
             launch_convert<double, float>(td.Lpost, tf.Lpost, c->n_int * rr, st);
@@ -356,11 +375,12 @@ mra_status finish_eval(mra_ctx* c) {
     for (int i = 0; i < c->n_timed; ++i) {
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, c->tev[2 * i], c->tev[2 * i + 1]));
-        const bool in_plan = i < (int)c->plan.size();
-        int kind = in_plan ? c->plan[i].kind : MRA_KERNEL_PREDICT;
+        const int pi = i < (int)c->timed_plan.size() ? c->timed_plan[i] : -1;
+        const bool in_plan = pi >= 0;
+        int kind = in_plan ? c->plan[pi].kind : MRA_KERNEL_PREDICT;
         s.timed_kind[i] = kind;
-        s.timed_level[i] = in_plan ? c->plan[i].level : -1;
-        s.timed_flop[i] = in_plan ? c->plan[i].flop : c->flop_predict_launch;
+        s.timed_level[i] = in_plan ? c->plan[pi].level : -1;
+        s.timed_flop[i] = in_plan ? c->plan[pi].flop : c->flop_predict_launch;
         s.timed_ms[i] = ms;
         s.ms_total += ms;
         if (kind == MRA_KERNEL_FIELDS) s.ms_fields += ms;
@@ -502,6 +522,7 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     t.queue = sh.queue;
     t.err = sh.err;
     t.factored = sh.factored;
+    t.active = nullptr;
     t.fuse_post = (prior_part && post_part) ? 1 : 0;
     int64_t uo = 0;
     for (int m = 0; m < kMaxLevels; ++m) t.u_off[m] = 0;
@@ -669,6 +690,9 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         }
     }
     for (long i = 0; i < n_int; ++i) h.factored[i] = (h.sub_hi[i] - h.sub_lo[i]) <= c->tf ? 1 : 0;
+    c->h_factored = h.factored;
+    c->h_sub_lo = h.sub_lo;
+    c->h_sub_hi = h.sub_hi;
     // slot of each dense region among the dense regions of its level: the dense
     // outputs (A~ slices, w~) of a level are stored compactly
     h.dslot.assign(n_int, -1);
@@ -678,6 +702,7 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
         for (long q = 0; q < cnt; ++q)
             if (!h.factored[s0 + q]) h.dslot[s0 + q] = k++;
     }
+    c->h_dslot = h.dslot;
     // work items of the finest kernel: a level M-3 region with its J sibling
     // groups when it holds at most 64 J observations (conditioning shared by
     // the groups), else each of its groups alone (load balance); for M = 2 the
@@ -865,6 +890,7 @@ mra_status mra_set_obs_values(mra_ctx* c, const double* y) {
 
 mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
     if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (c->shard_split) return fail(MRA_ERR_STATE, "the context is sharded: use mra_shard_* (or clear the sharding)");
     if (c->graph_exec) {
         CU(cudaGraphLaunch(c->graph_exec, c->stream));
         c->stats.graph_replays++;
@@ -883,6 +909,7 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
 mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
     if (!c) return fail(MRA_ERR_ARG, "NULL context");
     if (!c->have_pred) return fail(MRA_ERR_STATE, "the structure has no prediction locations");
+    if (c->shard_split) return fail(MRA_ERR_STATE, "prediction is not sharded: clear the sharding first");
     if (!(c->mixed_prior32 && c->mixed_finest32))
         return fail(MRA_ERR_STATE, "prediction needs the mixed path with both FP32 stages (MRA_MIXED_FP32)");
     if (c->graph_pred_exec) {
@@ -933,6 +960,7 @@ mra_status capture_one(mra_ctx* c, bool predict, cudaGraph_t* graph, cudaGraphEx
 
 mra_status mra_capture_graph(mra_ctx* c) {
     if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (c->shard_split) return fail(MRA_ERR_STATE, "sharded evaluations are not captured");
     if (!c->graph_exec) {
         mra_status s = capture_one(c, false, &c->graph, &c->graph_exec);
         if (s) return s;
@@ -942,6 +970,152 @@ mra_status mra_capture_graph(mra_ctx* c) {
         if (s) return s;
     }
     return MRA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sub-tree sharding
+// ---------------------------------------------------------------------------
+namespace {
+
+long shard_pow(int J, int e) { return level_count(J, e); }
+
+// doubles of the export record of one split-level region (see mra_b200.h)
+long shard_record_doubles(const mra_ctx* c, long q) {
+    const int s = c->shard_split, r = c->r;
+    const long i = level_start(c->J, s) + q;
+    const long rr = (long)r * r;
+    long n = 2;
+    if (c->h_factored[i]) {
+        const long rows = c->h_sub_hi[i] - c->h_sub_lo[i];
+        n += rows * (long)s * r + rows;
+    } else {
+        n += n_slices(s) * rr + (long)s * r;
+    }
+    for (int m = s; m <= c->M - 2; ++m) n += shard_pow(c->J, m - s);  // posterior terms of the sub-tree
+    n += shard_pow(c->J, c->M - 2 - s);                                 // finest terms of its groups
+    return n;
+}
+
+// copies between a record and the device buffers (to_device: import)
+mra_status shard_copy(mra_ctx* c, long q, double* rec, bool to_device) {
+    const int s = c->shard_split, r = c->r, J = c->J;
+    const long i = level_start(J, s) + q;
+    const long rr = (long)r * r;
+    DevTree<double>& t = c->td;
+    const cudaMemcpyKind k = to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    auto cp = [&](double* dev, double* host, long n) -> cudaError_t {
+        if (n <= 0) return cudaSuccess;
+        return to_device ? cudaMemcpy(dev, host, n * sizeof(double), k) : cudaMemcpy(host, dev, n * sizeof(double), k);
+    };
+    const double kind = c->h_factored[i] ? 1.0 : 0.0;
+    const long rows = c->h_sub_hi[i] - c->h_sub_lo[i];
+    if (to_device) {
+        if (rec[0] != kind || (kind == 1.0 && rec[1] != (double)rows))
+            return fail(MRA_ERR_ARG, "mra_shard_import: the record does not match this structure");
+    } else {
+        rec[0] = kind;
+        rec[1] = kind == 1.0 ? (double)rows : 0.0;
+    }
+    double* p = rec + 2;
+    if (kind == 1.0) {
+        const long lo = c->h_sub_lo[i];
+        CU(cp(t.Fbuf[s & 1] + lo * (long)s * r, p, rows * (long)s * r));
+        p += rows * (long)s * r;
+        CU(cp(t.fbuf[s & 1] + lo, p, rows));
+        p += rows;
+    } else {
+        const long slot = c->h_dslot[i];
+        CU(cp(t.aout[s & 1] + slot * n_slices(s) * rr, p, n_slices(s) * rr));
+        p += n_slices(s) * rr;
+        CU(cp(t.wout[s & 1] + slot * (long)s * r, p, (long)s * r));
+        p += (long)s * r;
+    }
+    for (int m = s; m <= c->M - 2; ++m) {
+        const long w = shard_pow(J, m - s);
+        CU(cp(t.dpost + level_start(J, m) + q * w, p, w));
+        p += w;
+    }
+    const long wg = shard_pow(J, c->M - 2 - s);
+    CU(cp(t.dfin + q * wg, p, wg));
+    return MRA_OK;
+}
+
+mra_status shard_run(mra_ctx* c, int phase) {
+    c->eval_phase = phase;
+    mra_status s = run_eval(c, false);
+    c->eval_phase = 0;
+    if (s) return s;
+    return finish_eval(c);
+}
+
+}  // namespace
+
+mra_status mra_shard_set(mra_ctx* c, int32_t split_level, const uint8_t* owned) {
+    if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (!owned) {
+        c->shard_split = 0;
+        c->td.active = nullptr;
+        return MRA_OK;
+    }
+    if (c->precision != MRA_PRECISION_FP64) return fail(MRA_ERR_ARG, "sharding runs the FP64 path only");
+    if (c->M < 4 || split_level < 1 || split_level > c->M - 3)
+        return fail(MRA_ERR_ARG, "the split level must be in [1, M-3] (M >= 4)");
+    const int J = c->J, s = split_level;
+    std::vector<int8_t> act(c->n_int, 1);
+    for (int m = s; m <= c->M - 2; ++m) {
+        const long s0 = level_start(J, m), cnt = level_count(J, m), w = shard_pow(J, m - s);
+        for (long q = 0; q < cnt; ++q) act[s0 + q] = owned[q / w] ? 1 : 0;
+    }
+    if (!c->d_active) {
+        cudaError_t e = cudaSuccess;
+        c->d_active = c->alloc<int8_t>(c->n_int, &e);
+        if (e) return fail(MRA_ERR_OOM, "device allocation failed: sharding mask");
+    }
+    CU(cudaMemcpy(c->d_active, act.data(), c->n_int, cudaMemcpyHostToDevice));
+    c->shard_split = s;
+    c->td.active = c->d_active;
+    return MRA_OK;
+}
+
+mra_status mra_shard_loglik_subtrees(mra_ctx* c) {
+    if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (!c->shard_split) return fail(MRA_ERR_STATE, "mra_shard_set first");
+    return shard_run(c, 1);
+}
+
+mra_status mra_shard_record_size(const mra_ctx* c, uint64_t region, uint64_t* n_doubles) {
+    if (!c || !n_doubles) return fail(MRA_ERR_ARG, "NULL argument");
+    if (!c->shard_split) return fail(MRA_ERR_STATE, "mra_shard_set first");
+    if ((long)region >= level_count(c->J, c->shard_split)) return fail(MRA_ERR_ARG, "region out of range");
+    *n_doubles = (uint64_t)shard_record_doubles(c, (long)region);
+    return MRA_OK;
+}
+
+mra_status mra_shard_export(mra_ctx* c, uint64_t region, double* record, uint64_t n_doubles) {
+    if (!c || !record) return fail(MRA_ERR_ARG, "NULL argument");
+    if (!c->shard_split) return fail(MRA_ERR_STATE, "mra_shard_set first");
+    if ((long)region >= level_count(c->J, c->shard_split)) return fail(MRA_ERR_ARG, "region out of range");
+    if ((long)n_doubles != shard_record_doubles(c, (long)region)) return fail(MRA_ERR_ARG, "record size mismatch");
+    CU(cudaStreamSynchronize(c->stream));
+    return shard_copy(c, (long)region, record, false);
+}
+
+mra_status mra_shard_import(mra_ctx* c, uint64_t region, const double* record, uint64_t n_doubles) {
+    if (!c || !record) return fail(MRA_ERR_ARG, "NULL argument");
+    if (!c->shard_split) return fail(MRA_ERR_STATE, "mra_shard_set first");
+    if ((long)region >= level_count(c->J, c->shard_split)) return fail(MRA_ERR_ARG, "region out of range");
+    if ((long)n_doubles != shard_record_doubles(c, (long)region)) return fail(MRA_ERR_ARG, "record size mismatch");
+    CU(cudaStreamSynchronize(c->stream));
+    return shard_copy(c, (long)region, const_cast<double*>(record), true);
+}
+
+mra_status mra_shard_loglik_top(mra_ctx* c, double* d_out, double* ll_out) {
+    if (!c) return fail(MRA_ERR_ARG, "NULL context");
+    if (!c->shard_split) return fail(MRA_ERR_STATE, "mra_shard_set first");
+    mra_status s = shard_run(c, 2);
+    if (d_out) *d_out = c->stats.d;
+    if (ll_out) *ll_out = c->stats.loglik;
+    return s;
 }
 
 mra_status mra_get_terms(mra_ctx* c, double* out, int32_t n_out) {
@@ -1018,6 +1192,7 @@ mra_status mra_sample_prior(mra_ctx* c, const double* z_int, const double* z_obs
     if (!c || !z_int || (!z_obs && c->n_obs) || (!y_out && c->n_obs)) return fail(MRA_ERR_ARG, "NULL argument");
     if (!(c->mixed_prior32 && c->mixed_finest32))
         return fail(MRA_ERR_STATE, "sampling needs the mixed path with both FP32 stages (MRA_MIXED_FP32)");
+    if (c->shard_split) return fail(MRA_ERR_STATE, "sampling is not sharded: clear the sharding first");
     // the prior factors (U of the finest level, L_Sigma) come from one evaluation
     mra_status s = run_eval(c, false);
     if (s) return s;

@@ -190,6 +190,7 @@ __global__ void __launch_bounds__(kCovThreads, 4) k_cov_level(Geom g, DevTree<T>
         const long q = b / (m + 1);
         const int j = (int)(b - q * (m + 1));
         const long i = s0 + loc0 + q;
+        if (skipped(t, i)) continue;
         long a = i;  // the ancestor of level j (the region itself for j == m)
         for (int l = m; l > j; --l) a = (a - 1) / t.J;
         cov_block<T, KIND>(g, t.pts, a * r, r, i * r, r, j == m, out + b * rr, r, stage);
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(kCovThreads, 4) k_cov_finest(Geom g, DevTree<T
         const int j = (int)(b - ploc * L);
         const long lo = t.obs_off[t.child_lo[ploc]];
         const int np = (int)(t.obs_off[t.child_hi[ploc]] - lo);
-        if (np == 0) continue;
+        if (np == 0 || skipped(t, s2 + ploc)) continue;
         long a = s2 + ploc;
         for (int l = m; l > j; --l) a = (a - 1) / t.J;
         cov_block<T, KIND>(g, t.pts, a * r, r, t.obs0 + lo, np, false, t.Bhat + lo * Lr + (long)j * r, Lr, stage);
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
     for (long q = blockIdx.x; q < nloc; q += gridDim.x) {
         const long loc = loc0 + q;
         const long i = s0 + loc;
+        if (skipped(t, i)) continue;
         long anc[kMaxLevels];
         {
             long c = i;
@@ -629,6 +631,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
         const bool unit = item < n_units;
         const long g_lo = unit ? item * t.J : item - n_units, g_hi = unit ? g_lo + t.J : g_lo + 1;
         const long ui = unit ? level_start(t.J, m - 1) + item : s2 + g_lo;  // region whose subtree is the item
+        if (skipped(t, ui)) continue;  // uniform: the item is the same for the whole CTA
         long anc[kMaxLevels];
         if (m > 0) {
             long c = unit ? ui : (ui - 1) / t.J;
@@ -750,6 +753,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
     const bool from_finest = m == t.M - 2;  // children are finest regions: rows of B^, y~
     for (long loc = blockIdx.x; loc < cnt; loc += gridDim.x) {
         const long i = s0 + loc;
+        if (skipped(t, i)) continue;
         double dterm = 0.0;
         if (from_finest) {
             const long lo = t.sub_lo[i];

@@ -32,6 +32,8 @@ struct DevTree {
     long n_fin_items;
     const int64_t* pred_order; // [J^(M-2)] level M-2 regions (local index), most expensive prediction work first
     const int8_t* factored;    // [n_int] 1: the region's posterior output is kept as F, f
+    const int8_t* active;      // [n_int] sub-tree sharding: 0 = the region belongs to another rank's
+                               // sub-tree and is skipped; nullptr: every region is computed
     const int64_t* dslot;      // [n_int] slot of a dense region among its level's dense regions (-1: factored)
     const int64_t* lsig_off;   // [n_fin+1] offsets of the n_k x n_k blocks
     const int64_t* pc_off;     // [n_fin+1] offsets of the n_k x n_p,k prediction blocks
@@ -85,6 +87,10 @@ __host__ __device__ inline long level_count(int J, int m) {
     return p;
 }
 __host__ __device__ inline long n_slices(int m) { return (long)m * (m + 1) / 2; }
+template <typename T>
+__device__ __forceinline__ bool skipped(const DevTree<T>& t, long region) {
+    return t.active && !t.active[region];
+}
 // slice index of block (j,k), j <= k < m, row-major over the upper triangle
 // (the order of class_approximation.cpp:62-73)
 __host__ __device__ inline long slice_index(int m, int j, int k) { return (long)j * m - (long)j * (j - 1) / 2 + (k - j); }
