@@ -80,6 +80,9 @@ def parse_args():
                    help="instead of the log-likelihood line: the mixed path against the FP64 path on the same "
                         "inputs, per stage (device time of each launch, error of each part of d), with the "
                         "observed values and with y = 0 (log-determinants alone)")
+    p.add_argument("--shard", action="store_true",
+                   help="with N ranks: one log-likelihood per step split over the ranks by sub-trees "
+                        "(strong scaling; shard.py) instead of N independent replicas")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -590,6 +593,69 @@ def mixed_report_arm(args):
     print(json.dumps(out))
 
 
+def shard_arm(args, world, rank, local):
+    """One log-likelihood per step over all ranks (sub-tree sharding, shard.py):
+    every rank evaluates its sub-trees, rank 0 gathers the split level's records,
+    finishes the top levels and broadcasts the result.  Strong scaling: the job
+    evaluates the same tree whatever N.  Timed with CUDA events on each rank's
+    current stream around the whole step (the library's work and the exchange),
+    synchronised on both sides, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from nonstationary_mra_b200 import api, replicas, shard, synth
+    torch.cuda.set_device(local)
+    api.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    cfg = synth.CONFIGS[args.config]
+    xy, pred, theta, md, st = make_problem(cfg)
+    sp = shard.plan(st, world)
+    ctx = api.Context(st, md)
+    # the values: rank 0 draws them (whole-tree evaluation) and broadcasts
+    y = draw_values(ctx, st, cfg.seed + 7) if rank == 0 else None
+    if world > 1:
+        box = [y]
+        dist.broadcast_object_list(box, src=0)
+        y = box[0]
+    ctx.set_obs_values(y)
+    ctx.set_theta()
+    for _ in range(max(args.warmup, 0)):
+        d, ll = shard.loglik(ctx, sp, rank, world)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    barrier()
+    with ClockSampler(local) as clk:
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            d, ll = shard.loglik(ctx, sp, rank, world)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+    barrier()
+    launches = ctx.shard_launches
+    ctx.close()
+    ms = replicas.max_over_ranks([ms], device="cuda")[0]
+    line = {"metric": METRIC, "value": args.steps / (ms * 1e-3), "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, y drawn from the MRA prior)",
+            "config": {"workload": workload_name(cfg), "parallelism": f"subtrees{world}", "split_level": sp.split,
+                       "subtrees_per_rank": [int((sp.owner == k).sum()) for k in range(world)],
+                       "estimated_load_imbalance": float(sp.load.max() / max(sp.load.mean(), 1e-300)),
+                       "loglik": ll, "d": d, "l2": "inputs larger than L2"},
+            "gpu_launches": launches * args.steps, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     if args.mixed_report:
@@ -610,6 +676,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             reference_arm(args)
+        return
+    if args.shard:
+        shard_arm(args, world, rank, local)
         return
     import torch
     import torch.distributed as dist

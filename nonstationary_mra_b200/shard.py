@@ -96,6 +96,7 @@ def loglik(ctx, sp: ShardPlan, rank: int = 0, world: int = 1, group=None):
     ctx.shard_set(sp.split, owned)
     try:
         ctx.shard_subtrees()
+        launches = ctx.stats()["kernel_launches"] if hasattr(ctx, "stats") else 0
         records = {int(q): ctx.shard_export(int(q)) for q in np.nonzero(owned)[0]}
         if world > 1:
             import torch.distributed as dist
@@ -114,6 +115,8 @@ def loglik(ctx, sp: ShardPlan, rank: int = 0, world: int = 1, group=None):
             if got != set(range(len(sp.owner))):
                 raise RuntimeError("a sub-tree record is missing")
             result = list(ctx.shard_top())
+            launches += ctx.stats()["kernel_launches"] if hasattr(ctx, "stats") else 0
+        ctx.shard_launches = launches  # kernels this rank launched for the evaluation
         if world > 1:
             import torch.distributed as dist
             dist.broadcast_object_list(result, src=0, group=group)
