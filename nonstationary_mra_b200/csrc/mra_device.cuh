@@ -281,16 +281,19 @@ __device__ __forceinline__ double rsqrt_fast(double x) {
 // One nonstationary straight-line entry from per-point quantities (see
 // fill_row_fast): row point (pc, ga, ca = sqrt(s1) b1 / scale^2 for PREF 1;
 // ssa, ba_h = b1 / scale^2 for PREF 0), column point (q, gq, ssbq = sqrt(s2) b2;
-// ssq, bq).
-template <int NU, int PREF>
+// ssq, bq).  F32SEED: reciprocal and inverse square root seeded in FP32
+// (rcp_fast / rsqrt_fast; more independent work per issue slot, for launches
+// that are issue-bound) or in FP64 (rcp_nr / rsqrt_nr; shorter dependent
+// chains, for fills that are latency-bound inside the region kernels).
+template <int NU, int PREF, bool F32SEED = false>
 __device__ __forceinline__ double cov_fast_entry(double pc0, double pc1, double pc2, double ga, double ca,
                                                  double ssa, double ba_h, double qx, double qy, double qz, double gq,
                                                  double ssbq, double ssq, double bq) {
     const double dx = qx - pc0, dy = qy - pc1, dz = qz - pc2;
     const double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
-    const double w = rcp_fast(ga + gq);  // 2 scale^2 / (b1^2 + b2^2)
-    const double u = d2 * w;             // h^2
-    const double h = u > 1e-300 ? u * rsqrt_fast(u) : 0.0;
+    const double w = F32SEED ? rcp_fast(ga + gq) : rcp_nr(ga + gq);  // 2 scale^2 / (b1^2 + b2^2)
+    const double u = d2 * w;                                            // h^2
+    const double h = u > 1e-300 ? u * (F32SEED ? rsqrt_fast(u) : rsqrt_nr(u)) : 0.0;
     const double em = exp_neg(h);
     const double m = NU == 3 ? (1.0 + h) * em : em;
     if (PREF == 1) return (ca * ssbq) * w * m;

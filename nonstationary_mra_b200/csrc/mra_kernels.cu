@@ -145,7 +145,7 @@ __device__ __forceinline__ void cov_block_fast(const PointSet& P, long a0, int n
 #pragma unroll 4
             for (int q = tc; q < qn; q += cols) {
                 const int qq = q0 + q;
-                double v = cov_fast_entry<NU, PREF>(pc0, pc1, pc2, ga, ca, ssa, ba_h, sx[q], sy[q], sz[q], sg[q],
+                double v = cov_fast_entry<NU, PREF, true>(pc0, pc1, pc2, ga, ca, ssa, ba_h, sx[q], sy[q], sz[q], sg[q],
                                                     PREF == 1 ? s4[q] : 0.0, PREF == 1 ? 0.0 : s4[q],
                                                     PREF == 1 ? 0.0 : s5[q]);
                 if (self && t == qq) v = diag;  // sigma^2 + tau^2 (evaluate_covariance.cpp:103,307)
@@ -197,31 +197,6 @@ __global__ void __launch_bounds__(kCovThreads, 4) k_cov_level(Geom g, DevTree<T>
     }
 }
 
-// The finest level's blocks against the ancestors, in their own launch before
-// k_finest_group: for every level M-2 region p (a sibling group: its finest
-// children's observations S_p are contiguous) and every level j = 0..M-2, the
-// block C(Q_{a_j}, S_p) (a_{M-2} = p) into the rows of B^ (obs-major, ld L r),
-// which the finest kernel then conditions in place
-// (...-loop-regions-at-finest-level-in-prior.cpp:116-160).
-template <typename T, int KIND>
-__global__ void __launch_bounds__(kCovThreads, 4) k_cov_finest(Geom g, DevTree<T> t) {
-    __shared__ double stage[7 * kCovChunk];
-    const int r = t.r, L = t.L, m = t.M - 2;
-    const long Lr = (long)L * r;
-    const long s2 = level_start(t.J, m), cnt2 = level_count(t.J, m);
-    const long nblocks = cnt2 * L;
-    for (long b = blockIdx.x; b < nblocks; b += gridDim.x) {
-        const long ploc = b / L;
-        const int j = (int)(b - ploc * L);
-        const long lo = t.obs_off[t.child_lo[ploc]];
-        const int np = (int)(t.obs_off[t.child_hi[ploc]] - lo);
-        if (np == 0 || skipped(t, s2 + ploc)) continue;
-        long a = s2 + ploc;
-        for (int l = m; l > j; --l) a = (a - 1) / t.J;
-        cov_block<T, KIND>(g, t.pts, a * r, r, t.obs0 + lo, np, false, t.Bhat + lo * Lr + (long)j * r, Lr, stage);
-    }
-}
-
 // Host-side dispatch of the covariance-block launches on the model's form.
 template <typename T>
 void launch_cov_level(const Geom& g, const DevTree<T>& t, int m, long loc0, long n, unsigned grid, cudaStream_t st) {
@@ -231,16 +206,6 @@ void launch_cov_level(const Geom& g, const DevTree<T>& t, int m, long loc0, long
         case 3: k_cov_level<T, 3><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
         case 4: k_cov_level<T, 4><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
         default: k_cov_level<T, 0><<<grid, kCovThreads, 0, st>>>(g, t, m, loc0, n, t.cbuf); break;
-    }
-}
-template <typename T>
-void launch_cov_finest(const Geom& g, const DevTree<T>& t, unsigned grid, cudaStream_t st) {
-    switch (cov_kind(g, sizeof(T) == 8)) {
-        case 1: k_cov_finest<T, 1><<<grid, kCovThreads, 0, st>>>(g, t); break;
-        case 2: k_cov_finest<T, 2><<<grid, kCovThreads, 0, st>>>(g, t); break;
-        case 3: k_cov_finest<T, 3><<<grid, kCovThreads, 0, st>>>(g, t); break;
-        case 4: k_cov_finest<T, 4><<<grid, kCovThreads, 0, st>>>(g, t); break;
-        default: k_cov_finest<T, 0><<<grid, kCovThreads, 0, st>>>(g, t); break;
     }
 }
 
@@ -644,9 +609,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
         const long ulo = t.sub_lo[ui];
         const int nu = (int)(t.sub_hi[ui] - ulo);
         if (m > 0 && nu > 0) {
-            // B^ holds C(Q_{a_j}, S) of every level (k_cov_finest); conditioned in place
+            // C(Q_{a_j}, S) of levels 0..M-3 for all observations of the unit, into B^
             T* Uf = t.Ufin + ulo * Lr;  // (L r) x nu, ld = L r
             T* Bh = t.Bhat + ulo * Lr;
+            long aoff[kMaxLevels];
+            for (int j = 0; j < m; ++j) aoff[j] = anc[j] * r;
+            fill_cov_blocks<T>(g, t.pts, aoff, m, r, t.obs0 + ulo, nu, false, Bh, Lr, r, sm);
             for (int j = 0; j < m; ++j) {
                 const long a = anc[j];
                 T* V = Bh + (long)j * r;  // V_j (kept: B^ is L_Sigma^{-1} V^T)
@@ -666,7 +634,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_finest_group(Geom g, DevTree<T>
             if (np > 0) {
                 // level M-2: the group's own parent p
                 T* Uf = t.Ufin + lo * Lr;
-                T* V = t.Bhat + lo * Lr + (long)m * r;  // C(Q_p, S) from k_cov_finest
+                T* V = t.Bhat + lo * Lr + (long)m * r;
+                const long ap = p * r;
+                fill_cov_blocks<T>(g, t.pts, &ap, 1, r, t.obs0 + lo, np, false, V, Lr, 0, sm);
                 if (m > 0) {
                     const T* Ua = t.U + t.u_off[m] + ploc * (long)m * rr;
                     gemm<T, true, false>(r, np, m * r, (T)-1, Ua, (long)m * r, Uf, Lr, (T)1, V, Lr, sm);
@@ -1013,12 +983,9 @@ int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cuda
 }
 template <typename T>
 int launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st) {
-    const long nb = level_count(t.J, t.M - 2) * t.L;
-    const long cov_grid = (long)grid * 16;
-    launch_cov_finest<T>(g, t, (unsigned)(nb < cov_grid ? nb : cov_grid), st);
     long cnt = t.n_fin_items;
     k_finest_group<T><<<(unsigned)(cnt < grid ? cnt : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, keep ? 1 : 0);
-    return 2;
+    return 1;
 }
 template <typename T>
 void launch_posterior_level(const Geom& g, const DevTree<T>& t, int m, int grid, bool keep, cudaStream_t st) {

@@ -126,8 +126,7 @@ void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const
 // of regions whose blocks fit t.cbuf; returns the number of kernels launched.
 template <typename T>
 int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st);
-// The finest level's covariance blocks against the ancestors, then the finest
-// groups; returns the number of kernels launched (2).
+// The finest groups; returns the number of kernels launched (1).
 template <typename T>
 int launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st);
 template <typename T>
