@@ -396,6 +396,8 @@ mra_status finish_eval(mra_ctx* c) {
     s.bytes_device = c->bytes;
     s.kernel_launches = c->last_launches;
     s.bad_region = -1;
+    if (err[0] == MRA_ERR_TIMEOUT)
+        return fail(MRA_ERR_TIMEOUT, "a bounded device-side wait gave up");
     if (err[0] != 0) {
         s.bad_region = (int64_t)(unsigned)err[1] | ((int64_t)err[2] << 31);
         char buf[128];
