@@ -70,6 +70,10 @@ def parse_args():
                    help="instead of the log-likelihood line: fit wall-time of the plain optimizer vs the "
                         "surrogate-assisted one (19 nonstationary parameters, c2 layout)")
     p.add_argument("--fit-evals", type=int, default=2000)
+    p.add_argument("--fit-curve", action="store_true",
+                   help="with --fit: the best log-likelihood against exact evaluations and wall time of the plain "
+                        "optimizer and of the surrogate-assisted one for several training-set sizes")
+    p.add_argument("--fit-ntrain", default="100,200,400", help="training-set sizes of --fit-curve")
     p.add_argument("--sweep", action="store_true",
                    help="instead of the log-likelihood line: the scaling sweep n in {1M, 2M, 4M} x M in "
                         "{10, 11, 12} x r in {32, 64, 128} (one JSON line per case)")
@@ -354,6 +358,54 @@ def reference_arm(args):
                 e2e={"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     line["config"]["seconds_per_step"] = secs
     print(json.dumps(line))
+
+
+def fit_curve_arm(args):
+    """The surrogate's effect, measured: the best exact log-likelihood reached
+    after k exact evaluations (and the wall time), for the plain optimizer and
+    for the surrogate-assisted optimizer trained on its first n_train
+    evaluations, n_train from --fit-ntrain; the same seeded start and bounds as
+    --fit."""
+    from nonstationary_mra_b200 import api, synth
+    from nonstationary_mra_b200.fit import FitConfig, NonstationaryObjective, fit_plain, fit_surrogate
+    cfg = synth.CONFIGS["c2" if args.config == "c3" else args.config]
+    xy, pred, theta, md, st = make_problem(cfg)
+    ctx = api.Context(st, md)
+    y = draw_values(ctx, st, cfg.seed + 7)
+    ctx.set_obs_values(y)
+    ctx.set_theta()
+    ctx.capture_graph()
+    rng = np.random.Generator(np.random.PCG64(cfg.seed + 11))
+    th0 = np.concatenate([0.3 * rng.standard_normal(9), cfg.range_sd * rng.standard_normal(9), [np.log(0.1)]])
+    lo = np.concatenate([-2.5 * np.ones(18), [np.log(1e-3)]])
+    hi = np.concatenate([2.5 * np.ones(18), [0.0]])
+    icpt = (0.0, float(np.log(0.1)))
+    marks = [k for k in (50, 100, 200, 300, 400, 500, 750, 1000, 1250, 1500, 1750, 2000, 2500, 3000)
+             if k <= args.fit_evals]
+
+    def curve(trace):
+        best = np.maximum.accumulate(np.asarray(trace.loglik))
+        return {str(k): {"loglik": float(best[k - 1]), "seconds": float(trace.seconds[k - 1])}
+                for k in marks if k <= len(best)}
+
+    plain = NonstationaryObjective(ctx, *icpt)
+    fit_plain(plain, th0, lo, hi, FitConfig(max_evals=args.fit_evals))
+    L = plain.trace.best_loglik()
+    target = L - 1e-6 * abs(L)
+    out = {"metric": "surrogate-assisted fitting: best exact loglik vs exact evaluations",
+           "workload": workload_name(cfg) + ", theta = 9 log-sigma + 9 log-range + log tau^2",
+           "seconds_per_eval": float(np.median(np.diff(plain.trace.seconds))),
+           "plain": {"final_loglik": L, "evals": len(plain.trace.loglik), "curve": curve(plain.trace),
+                     "evals_to_final": plain.trace.evals_to_reach(target)}}
+    for nt in [int(v) for v in args.fit_ntrain.split(",") if v]:
+        sur = NonstationaryObjective(ctx, *icpt)
+        _, Ls, info = fit_surrogate(sur, th0, lo, hi, FitConfig(max_evals=args.fit_evals, n_train=nt))
+        out[f"surrogate_ntrain{nt}"] = {"final_loglik": Ls, "evals": info["evals"], "proposals": info["proposals"],
+                                        "accepted": info["accepted"], "curve": curve(sur.trace),
+                                        "evals_to_plain_final": sur.trace.evals_to_reach(target),
+                                        "seconds_to_plain_final": sur.trace.time_to_reach(target)}
+    ctx.close()
+    print(json.dumps(out))
 
 
 def fit_arm(args):
@@ -662,7 +714,10 @@ def main():
         mixed_report_arm(args)
         return
     if args.fit:
-        fit_arm(args)
+        if args.fit_curve:
+            fit_curve_arm(args)
+        else:
+            fit_arm(args)
         return
     if args.predict:
         predict_arm(args)
