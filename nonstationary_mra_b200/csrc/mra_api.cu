@@ -166,7 +166,7 @@ mra_status upload(void* dst, const void* src, size_t bytes, cudaStream_t st) {
 // Host-side description of the tree used for sizing, scheduling and FLOP counts.
 struct HostTree {
     std::vector<int64_t> nfin, npred, obs_off, pred_off, fin_anc, pred_order, lsig_off, pc_off;
-    std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi, dslot;
+    std::vector<int64_t> child_lo, child_hi, par_order, sub_lo, sub_hi, dslot, post_order;
     std::vector<int8_t> factored;
 };
 
@@ -274,7 +274,7 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     const bool mixed = c->precision == MRA_PRECISION_MIXED;
     DevTree<double>& td = c->td;
     DevTree<float>& tf = c->tf32;
-    CU(cudaMemsetAsync(td.queue, 0, 4 * sizeof(int), st));
+    CU(cudaMemsetAsync(td.queue, 0, kQueueCounters * sizeof(int), st));
     CU(cudaMemsetAsync(td.err, 0, 4 * sizeof(int), st));
     const long np_all = c->n_int * c->r + c->n_obs + c->n_pred;
     const long rr = (long)c->r * c->r;
@@ -432,6 +432,7 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     t.pc_off = idx[5]; t.child_lo = idx[6]; t.child_hi = idx[7]; t.par_order = idx[8]; t.sub_lo = idx[9];
     t.sub_hi = idx[10];
     t.dslot = idx[11];
+    t.post_order = idx[12];
     t.n_fin_items = (long)h.par_order.size();
     // sizes of the level-parity buffers
     size_t aout_sz[2] = {1, 1}, wout_sz[2] = {1, 1}, F_sz[2] = {1, 1}, f_sz[2] = {1, 1};
@@ -487,14 +488,20 @@ mra_status setup_tree(mra_ctx* c, DevTree<T>& t, const HostTree& h, const PointS
     }
     TALLOC(t.ws, T, (long)c->grid * t.ws_stride);
     // covariance blocks of the prior levels: all of a level's blocks when they
-    // fit MRA_COV_BUF_MB (default 2048 MB), else the level runs in chunks of
-    // regions (a smaller buffer is tried when the first allocation fails)
+    // fit MRA_COV_BUF_MB (default 2048 MB; 8192 MB for the FP64 path when more
+    // than 24 GB stay free: fewer chunks, fewer drained launches), else the
+    // level runs in chunks of regions (a smaller buffer is tried when the first
+    // allocation fails)
     t.cbuf = nullptr;
     t.cbuf_elems = 0;
     if (prior_part) {
         long need = 0;
         for (int m = 0; m <= M - 2; ++m) need = std::max(need, level_count(J, m) * (long)(m + 1) * rr);
         long cap_mb = 2048;
+        size_t free_b = 0, total_b = 0;
+        if (sizeof(T) == 8 && c->precision == MRA_PRECISION_FP64 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+            free_b > (size_t)24 << 30)
+            cap_mb = 8192;
         if (const char* e = std::getenv("MRA_COV_BUF_MB")) cap_mb = std::max(1L, std::atol(e));
         long elems = std::min(need, cap_mb * (1L << 20) / (long)sizeof(T));
         const long floor_elems = std::min(need, (long)(M - 1) * rr * c->grid);  // one region per CTA slot
@@ -705,6 +712,35 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
             if (!h.factored[s0 + q]) h.dslot[s0 + q] = k++;
     }
     c->h_dslot = h.dslot;
+    // posterior work items of each level, most expensive first: a factored
+    // region costs about n^2 (m r) for its n observations, a dense one the
+    // accumulation of its factored children ((m+1) r)^2 per row plus its
+    // r^3-sized step
+    h.post_order.assign(n_int, 0);
+    for (int mm = 0; mm <= M - 2; ++mm) {
+        const long s0 = level_start(J, mm), cnt = level_count(J, mm);
+        std::vector<double> cost(cnt);
+        const double w = (double)(mm + 1) * r;
+        for (long q = 0; q < cnt; ++q) {
+            const long i = s0 + q;
+            const double n = (double)(h.sub_hi[i] - h.sub_lo[i]);
+            if (h.factored[i]) {
+                cost[q] = n * n * (double)(mm * r) + n * (double)r * r;
+            } else {
+                double rows = 0.0;
+                if (mm == M - 2) rows = n;
+                else
+                    for (int cc = 1; cc <= J; ++cc) {
+                        const long ch = i * J + cc;
+                        if (h.factored[ch]) rows += (double)(h.sub_hi[ch] - h.sub_lo[ch]);
+                    }
+                cost[q] = rows * w * w / 2 + (double)r * r * r * (0.5 * mm * mm + mm + 1.0);
+            }
+        }
+        for (long q = 0; q < cnt; ++q) h.post_order[s0 + q] = q;
+        std::stable_sort(h.post_order.begin() + s0, h.post_order.begin() + s0 + cnt,
+                         [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    }
     // work items of the finest kernel: a level M-3 region with its J sibling
     // groups when it holds at most 64 J observations (conditioning shared by
     // the groups), else each of its groups alone (load balance); for M = 2 the
@@ -757,11 +793,11 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     }
     double* y = c->alloc<double>(n_obs, &ce);
     if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: y"));
-    const std::vector<int64_t>* tabs[12] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.pred_order, &h.lsig_off,
+    const std::vector<int64_t>* tabs[13] = {&h.obs_off, &h.pred_off, &h.fin_anc, &h.pred_order, &h.lsig_off,
                                             &h.pc_off, &h.child_lo, &h.child_hi, &h.par_order, &h.sub_lo, &h.sub_hi,
-                                            &h.dslot};
-    int64_t* idx[12];
-    for (int q = 0; q < 12; ++q) {
+                                            &h.dslot, &h.post_order};
+    int64_t* idx[13];
+    for (int q = 0; q < 13; ++q) {
         idx[q] = c->alloc<int64_t>(tabs[q]->size(), &ce);
         if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: index tables"));
         mra_status u = upload(idx[q], tabs[q]->data(), tabs[q]->size() * sizeof(int64_t), c->stream);
@@ -799,7 +835,7 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     if (!ce) sh.dfin = c->alloc<double>(cnt2, &ce);
     if (!ce) sh.mean = c->alloc<double>(n_pred, &ce);
     if (!ce) sh.var = c->alloc<double>(n_pred, &ce);
-    if (!ce) sh.queue = c->alloc<int>(4, &ce);
+    if (!ce) sh.queue = c->alloc<int>(kQueueCounters, &ce);
     if (!ce) sh.err = c->alloc<int>(4, &ce);
     if (!ce) sh.factored = c->alloc<int8_t>(n_int, &ce);
     if (ce) return bail(fail(MRA_ERR_OOM, "device allocation failed: shared vectors"));

@@ -457,6 +457,16 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool p
     const int n = pred ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
 }
+// Bulk prefetch into L2 of the 16-byte aligned part of [p, p + bytes) (the
+// instruction takes a 16-byte aligned address and a multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned long bytes) {
+    const unsigned long a = ((unsigned long)p + 15) & ~15ul, b = ((unsigned long)p + bytes) & ~15ul;
+    if (b <= a || b - a > 0xffffffffull) return;
+    asm volatile(
+        "{\n\t.reg .u64 ga;\n\tcvta.to.global.u64 ga, %0;\n\tcp.async.bulk.prefetch.L2.global [ga], %1;\n\t}\n" ::"l"(a),
+        "r"((unsigned)(b - a))
+        : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -1128,13 +1138,47 @@ __device__ inline int potrf_small(int n, double* A, long lda, LaSmem<double>& sm
     return sm.flag;
 }
 
+// FP64 Cholesky with the inverse of the factor for 64 < n <= 128, as a 2 x 2
+// block factorization around potrf_small (64 + n2 with n2 = n - 64):
+//   L11 = chol(A11), X11 = L11^{-1};  L21 = A21 X11^T;  A22 -= L21 L21^T;
+//   L22 = chol(A22), X22 = L22^{-1};  X21 = -X22 (L21 X11)
+// so that everything but the two diagonal factorizations runs as products on
+// the tensor pipe.  A and inv get zeros above the diagonal.  Returns 0 or the
+// 1-based index of the first bad pivot; logdet (thread 0) = 2 sum log L_ii.
+__device__ inline int potrf_mid(int n, double* A, long lda, LaSmem<double>& sm, double* logdet, double* inv,
+                                long ldinv) {
+    const int n2 = n - 64;
+    double ld1 = 0.0, ld2 = 0.0;
+    const int info1 = potrf_small(64, A, lda, sm, &ld1, inv, ldinv);
+    double* A21 = A + 64;
+    double* A22 = A + 64 + 64 * lda;
+    double* X21 = inv + 64;
+    double* X22 = inv + 64 + 64 * ldinv;
+    // L21 = A21 X11^T in place (a single output tile reads all of A21 first)
+    gemm<double, false, true, true>(n2, 64, 64, 1.0, A21, lda, inv, ldinv, 0.0, A21, lda, sm);
+    gemm<double, false, true>(n2, n2, 64, -1.0, A21, lda, A21, lda, 1.0, A22, lda, sm);
+    const int info2 = potrf_small(n2, A22, lda, sm, &ld2, X22, ldinv);
+    gemm<double, false, false>(n2, 64, 64, 1.0, A21, lda, inv, ldinv, 0.0, X21, ldinv, sm);
+    gemm<double, false, false, true>(n2, 64, n2, -1.0, X22, ldinv, X21, ldinv, 0.0, X21, ldinv, sm);
+    for (int e = threadIdx.x; e < 64 * n2; e += kThreads) {
+        const int i = e & 63, j = 64 + (e >> 6);
+        A[i + (long)j * lda] = 0.0;
+        inv[i + (long)j * ldinv] = 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && logdet) *logdet = ld1 + ld2;
+    return info1 ? info1 : (info2 ? info2 + 64 : 0);
+}
+
 // In-place lower Cholesky (see potrf_blocked); FP64 matrices up to 64 go
-// through potrf_small.  With `inv`, L^{-1} is also written there (ld ldinv).
+// through potrf_small, and up to 128 through potrf_mid when the inverse is
+// asked for.  With `inv`, L^{-1} is also written there (ld ldinv).
 template <typename T>
 __device__ inline int potrf_lower(int n, T* A, long lda, LaSmem<T>& sm, double* logdet, T* inv = nullptr,
                                   long ldinv = 0) {
     if constexpr (sizeof(T) == 8) {
         if (n <= 64) return potrf_small(n, A, lda, sm, logdet, inv, ldinv);
+        if (n <= 128 && inv) return potrf_mid(n, A, lda, sm, logdet, inv, ldinv);
     }
     const int info = potrf_blocked(n, A, lda, sm, logdet);
     if (inv) {

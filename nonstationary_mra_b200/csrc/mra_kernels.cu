@@ -247,6 +247,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             const long a = anc[j];
             const T* Cj = Cq + j * rr;
             const T* Vj = Cj;  // level 0 has nothing to condition on
+            // the next covariance block (or the self block) into L2 while this step's products run
+            if (threadIdx.x == 0) prefetch_l2(Cj + rr, rr * sizeof(T));
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
                 gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm, Cj, r);
@@ -291,14 +293,14 @@ __device__ __noinline__ void factored_step(const DevTree<T>& t, int m, long i, i
     const T* Li = t.Lprior + i * rr;
     T* Y = ws;                  // r x n
     T* S = ws + (long)r * n;    // n x n
-    T* Rinv = S + (long)n * n;  // n x n (n <= 64)
+    T* Rinv = S + (long)n * n;  // n x n (n <= 128)
     // Y = L_i^{-1} F_m^T as a product with the stored inverse of the prior factor
     gemm_call<T, false, false>(r, n, r, (T)1, t.Pinv + i * rr, r, F + mr, ldF, (T)0, Y, r, sm);
     gemm_call<T, true, false>(n, n, r, (T)1, Y, r, Y, r, (T)0, S, n, sm);
     for (int q = threadIdx.x; q < n; q += kThreads) S[q + (long)q * n] += (T)1;
     __syncthreads();
     double ld = 0.0;
-    const bool small = sizeof(T) == 8 && n <= 64;
+    const bool small = sizeof(T) == 8 && n <= 128;
     int info = potrf_lower<T>(n, S, n, sm, &ld, small ? Rinv : nullptr, n);
     double* fp = m > 0 ? fo : wsd;
     double part = 0.0;
@@ -721,7 +723,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_posterior_level(Geom g, DevTree
     const T* ain = t.aout[(m + 1) & 1];
     const double* win = t.wout[(m + 1) & 1];
     const bool from_finest = m == t.M - 2;  // children are finest regions: rows of B^, y~
-    for (long loc = blockIdx.x; loc < cnt; loc += gridDim.x) {
+    // regions taken from a shared counter, most expensive first (the clustered
+    // regions' dense steps cost tens of factored ones)
+    __shared__ long s_loc;
+    for (;;) {
+        __syncthreads();  // every thread has read the previous s_loc
+        if (threadIdx.x == 0) {
+            const int q = atomicAdd(&t.queue[kQueuePost + m], 1);
+            s_loc = q < cnt ? t.post_order[s0 + q] : -1;
+        }
+        __syncthreads();
+        const long loc = s_loc;
+        if (loc < 0) break;
         const long i = s0 + loc;
         if (skipped(t, i)) continue;
         double dterm = 0.0;

@@ -31,6 +31,8 @@ struct DevTree {
                                // v < J^(M-3) is the level M-3 unit v, else the level M-2 group v - J^(M-3)
     long n_fin_items;
     const int64_t* pred_order; // [J^(M-2)] level M-2 regions (local index), most expensive prediction work first
+    const int64_t* post_order; // [n_int] per level m, at level_start(m): the level's regions (local index),
+                               // most expensive posterior step first
     const int8_t* factored;    // [n_int] 1: the region's posterior output is kept as F, f
     const int8_t* active;      // [n_int] sub-tree sharding: 0 = the region belongs to another rank's
                                // sub-tree and is skipped; nullptr: every region is computed
@@ -72,9 +74,13 @@ struct DevTree {
     double* mean;              // [n_pred]
     double* var;               // [n_pred]
     // bookkeeping
-    int* queue;                // work-queue counters
+    int* queue;                // work-queue counters (kQueueCounters, zeroed before every evaluation):
+                               // [0] finest items, [1] prediction items, [kQueuePost + m] posterior level m
     int* err;                  // [0]: status, [1]: region (low), [2]: region (high)
 };
+
+constexpr int kQueuePost = 4;
+constexpr int kQueueCounters = kQueuePost + kMaxLevels;
 
 __host__ __device__ inline long level_start(int J, int m) {
     long s = 0, p = 1;
