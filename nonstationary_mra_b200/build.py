@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -79,10 +80,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
                     "-I", os.path.join(ROOT, "include")]
     if verbose:
         flags += ["-Xptxas", "-v"]
-    for src in sources():
+    def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [nvcc()] + flags + ["-c", src, "-o", obj]
-        res = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the translation units compile independently: one nvcc per source at once
+    with ThreadPoolExecutor(max_workers=len(CU_SOURCES)) as pool:
+        results = list(pool.map(compile_one, sources()))
+    for src, (obj, res) in zip(sources(), results):
         if res.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{res.stderr}")
         if verbose and res.stderr:

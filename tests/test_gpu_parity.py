@@ -98,6 +98,8 @@ RANDOM_CASES = [
     (4, 4, 4, 9, 900, 50, False, 1, False),      # stationary
     (5, 2, 7, 4, 700, 80, True, 3, True),        # deep tree
     (6, 4, 5, 16, 3000, 200, True, 3, True),     # finest work items both batched and split; children up to 230
+    (8, 4, 5, 16, 1200, 60, False, 3, True),     # finest children of about 5 observations: one warp per child
+    (9, 4, 5, 12, 1500, 50, True, 1, True),      # clustered: per-warp, grouped and per-child paths side by side
 ]
 
 
