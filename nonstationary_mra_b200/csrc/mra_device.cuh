@@ -577,6 +577,88 @@ __device__ inline void gemm_f64(int M, int N, int K, double alpha, const double*
     __syncthreads();
 }
 
+// 16-byte asynchronous global -> shared copy through L2 only (not L1); both
+// addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(double* dst, const double* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// gemm_f64 for whole tiles (M % 64 == 0, N % (16 NW) == 0, K % 32 == 0) with
+// 16-byte aligned operand rows (aligned A and B, even lda and ldb): the same
+// tiles, the same shared-memory layout and the same per-element K order, hence
+// bitwise the same results, with the operands staged in pairs of elements by
+// 16-byte copies through L2 only -- half the copy instructions and no L1
+// allocation.
+template <bool TA, bool TB, int NW>
+__device__ inline void gemm_f64_wide(int M, int N, int K, double alpha, const double* A, long lda, const double* B,
+                                     long ldb, double beta, double* C, long ldc, LaSmem<double>& sm,
+                                     const double* Cin, long ldcin) {
+    constexpr int W = 16 * NW;
+    constexpr int WM = 8 / NW;
+    constexpr int QA = 64 * TK64 / 2 / kThreads;  // A pairs per thread per slab (4)
+    constexpr int QB = W * TK64 / 2 / kThreads;   // B pairs per thread per slab (NW)
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int wm = (w % WM) * 8 * NW, wn = (w / WM) * 16;
+    for (int m0 = 0; m0 < M; m0 += 64) {
+        for (int n0 = 0; n0 < N; n0 += W) {
+            AccD<NW> acc;
+#pragma unroll
+            for (int i = 0; i < NW; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) acc.v[i][j][0] = acc.v[i][j][1] = 0.0;
+            auto issue = [&](int k0, int stage) {
+                double* sA = sm.A[stage];
+                double* sB = sm.B[stage];
+#pragma unroll
+                for (int q = 0; q < QA; ++q) {
+                    const int e = tid + q * kThreads;
+                    // TA: pair (i, k..k+1) of A[k + i lda]; else pair (i..i+1, k) of A[i + k lda]
+                    const int i = TA ? e / (TK64 / 2) : 2 * (e % 32), k = TA ? 2 * (e % (TK64 / 2)) : e / 32;
+                    const double* src = TA ? A + (k0 + k) + (long)(m0 + i) * lda : A + (m0 + i) + (long)(k0 + k) * lda;
+                    cp_async16(sA + (TA ? i * KS64 + k : k * RS64 + i), src);
+                }
+#pragma unroll
+                for (int q = 0; q < QB; ++q) {
+                    const int e = tid + q * kThreads;
+                    // TB: pair (k, j..j+1) of B[j + k ldb]; else pair (k..k+1, j) of B[k + j ldb]
+                    const int j = TB ? 2 * (e % (W / 2)) : e / (TK64 / 2), k = TB ? e / (W / 2) : 2 * (e % (TK64 / 2));
+                    const double* src = TB ? B + (n0 + j) + (long)(k0 + k) * ldb : B + (k0 + k) + (long)(n0 + j) * ldb;
+                    cp_async16(sB + (TB ? k * RS64 + j : j * KS64 + k), src);
+                }
+                cp_async_commit();
+            };
+            issue(0, 0);
+            int stage = 0;
+            for (int k0 = 0; k0 < K; k0 += TK64, stage ^= 1) {
+                if (k0 + TK64 < K) {
+                    issue(k0 + TK64, stage ^ 1);
+                    cp_async_wait<1>();
+                } else {
+                    cp_async_wait<0>();
+                }
+                __syncthreads();
+                warp_step_f64<TA, TB, NW>(acc, sm.A[stage], sm.B[stage], wm, wn, lane);
+                __syncthreads();
+            }
+            const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+            for (int i = 0; i < NW; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int r = m0 + wm + 8 * i + g, c = n0 + wn + 8 * j + 2 * t;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        double* p = C + r + (long)(c + h) * ldc;
+                        const double* q = Cin ? Cin + r + (long)(c + h) * ldcin : p;
+                        *p = beta == 0.0 ? alpha * acc.v[i][j][h] : alpha * acc.v[i][j][h] + beta * *q;
+                    }
+                }
+        }
+    }
+    __syncthreads();
+}
+
 // ---- FP32 storage (mixed path): 3xTF32 products, 64 x 64 tiles, K slabs of 16
 struct AccF {
     float v[2][2][4];  // 2 (m16) x 2 (n8) fragments of m16n8
@@ -801,6 +883,25 @@ __device__ inline void trsm_right_lower_trans(int rows, int n, const T* L, long 
             gemm<T, false, true>(rows, n - b0 - nb, nb, (T)-1, B + (long)b0 * ldb, ldb, L + (b0 + nb) + (long)b0 * ldl,
                                  ldl, (T)1, B + (long)(b0 + nb) * ldb, ldb, sm);
     }
+}
+
+// gemm with the operand staging of gemm_f64_wide where the product qualifies
+// (FP64, whole tiles, 16-byte aligned rows), else gemm; the results are bitwise
+// the same either way.
+template <typename T, bool TA, bool TB>
+__device__ inline void gemm_wide(int M, int N, int K, T alpha, const T* A, long lda, const T* B, long ldb, T beta,
+                                 T* C, long ldc, LaSmem<T>& sm, const T* Cin = nullptr, long ldcin = 0) {
+    if constexpr (sizeof(T) == 8) {
+        const int nw = c_gemm_nw[N <= 16 ? 0 : (N <= 32 ? 1 : 2)];
+        if (M > 0 && K > 0 && M % 64 == 0 && N % (16 * nw) == 0 && K % TK64 == 0 && lda % 2 == 0 && ldb % 2 == 0 &&
+            (((unsigned long)A | (unsigned long)B) & 15ul) == 0) {
+            if (nw == 1) gemm_f64_wide<TA, TB, 1>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
+            else if (nw == 2) gemm_f64_wide<TA, TB, 2>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
+            else gemm_f64_wide<TA, TB, 4>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
+            return;
+        }
+    }
+    gemm<T, TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, sm, Cin, ldcin);
 }
 
 // Solves L x = b for one right-hand side entirely in FP64 (the vectors that feed

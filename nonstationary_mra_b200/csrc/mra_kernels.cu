@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_prior_level(Geom g, DevTree<T> 
             if (threadIdx.x == 0) prefetch_l2(Cj + rr, rr * sizeof(T));
             if (j > 0) {
                 const T* Ua = t.U + t.u_off[j] + (a - level_start(t.J, j)) * (long)j * rr;
-                gemm<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm, Cj, r);
+                gemm_wide<T, true, false>(r, r, j * r, (T)-1, Ua, (long)j * r, Ui, mr, (T)1, V, r, sm, Cj, r);
                 Vj = V;
             }
             // U_{i,j} = L_a^{-1} V as a product with the stored inverse
