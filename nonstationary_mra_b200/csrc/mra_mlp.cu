@@ -5,6 +5,9 @@
 // One kernel does the forward pass, the backward pass and the per-CTA
 // gradient sums over a grid-strided set of 16-sample tiles; a second kernel
 // adds the per-CTA sums in a fixed order (deterministic) and applies Adam.
+// Predictions without input gradients (the screening of candidate parameter
+// vectors) run k_mlp_forward_tc instead, whose 128 x 128 layer is a
+// tcgen05.mma product in tensor memory.
 // Thread h of a CTA owns hidden unit h: row h of W2 sits in its registers for
 // the forward product, and the backward product through W2 reads the BF16
 // copy of W2 in shared memory column-wise (consecutive threads, consecutive
@@ -275,6 +278,186 @@ __global__ void k_mlp_sync_bf16(long P, const float* master, __nv_bfloat16* W1b,
     else if (p >= ow3 && p < ob3) w3b[p - ow3] = __float2bfloat16_rn(w);
 }
 
+// ---------------------------------------------------------------------------
+// Forward pass on the 5th-generation tensor cores (prediction without input
+// gradients).  One CTA of 128 threads takes tiles of 128 samples, thread t =
+// sample t of the tile = TMEM lane t:
+//   layer 1 (n_in x 128, small) on the FP32 cores, exactly as k_mlp_pass;
+//   layer 2 (128 x 128 x 128) as tcgen05.mma kind::tf32 with the product in
+//     tensor memory: a1 is split into a TF32 high part and the FP32 remainder
+//     (a1 = hi + lo, hi exact in TF32), W2 is BF16 and hence exact in TF32, so
+//     hi W2^T + lo W2^T is FP32-accurate (the remainder's own truncation to TF32
+//     costs at most 2^-21 |a1|);
+//   the output layer on the FP32 cores from the product read back by tcgen05.ld.
+// Operands sit in shared memory in the canonical K-major layout without
+// swizzle: 8-row x 16-byte core matrices, the two core matrices of one MMA's K
+// slice 128 bytes apart (leading byte offset), consecutive 8-row groups 4096
+// bytes apart (stride byte offset).  One thread issues the MMAs and commits
+// them to an mbarrier; the others wait on it with a bounded spin.
+constexpr int TC_M = 128;                    // samples per tile = MMA M = TMEM lanes
+constexpr unsigned TC_LBO = 128, TC_SBO = 4096;
+constexpr long kTcSpin = 1L << 24;           // bounded waits (about a second)
+
+struct TcSmem {
+    float Ahi[TC_M * H];                     // 64 KB each, canonical K-major layout
+    float Alo[TC_M * H];
+    float W2f[H * H];                        // rows = output units
+    __nv_bfloat16 W1t[MAXD * H];             // layer 1 weights [d][h]
+    float b1[H], b2[H], w3[H];
+    unsigned long long bar;                  // MMA completion
+    unsigned tmem_base;
+    int abort;
+};
+
+// element (row, k) of a 128-row, 128-deep K-major tile of 4-byte elements
+__device__ __forceinline__ int tc_idx(int row, int k) {
+    return (row >> 3) * (int)(TC_SBO / 4) + (k >> 2) * (int)(TC_LBO / 4) + (row & 7) * 4 + (k & 3);
+}
+__device__ __forceinline__ unsigned tc_smem(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// shared-memory matrix descriptor: start, leading / stride byte offsets (>> 4),
+// descriptor version 1 (bits 46-47), no swizzle
+__device__ __forceinline__ unsigned long long tc_desc(unsigned addr) {
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((TC_LBO >> 4) & 0x3FFF) << 16) |
+           ((unsigned long long)((TC_SBO >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2),
+// both K-major, N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
+constexpr unsigned kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(H >> 3) << 17) | ((unsigned)(TC_M >> 4) << 24);
+
+// D[tmem] (+)= A B^T for one K slice of 8, A and B given by their descriptors
+__device__ __forceinline__ void tc_mma(unsigned tmem, unsigned long long adesc, unsigned long long bdesc, bool acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"((unsigned)acc)
+        : "memory");
+}
+__device__ __forceinline__ bool tc_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(tc_smem(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld32(unsigned taddr, float (&v)[32]) {
+    unsigned r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// y = MLP(x) for a.N samples (a.Y); *err = 1 if a bounded wait gave up.
+__global__ void __launch_bounds__(TC_M, 1) k_mlp_forward_tc(MlpArgs a, int* err) {
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, D = a.D;
+    for (int e = tid; e < H * H; e += TC_M) sm.W2f[tc_idx(e / H, e % H)] = __bfloat162float(a.W2b[e]);
+    for (int e = tid; e < H * D; e += TC_M) sm.W1t[(e % D) * H + e / D] = a.W1b[e];
+    for (int h = tid; h < H; h += TC_M) {
+        sm.b1[h] = a.master[a.b1 + h];
+        sm.b2[h] = a.master[a.b2 + h];
+        sm.w3[h] = __bfloat162float(a.w3b[h]);
+    }
+    if (tid == 0) {
+        sm.abort = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(tc_smem(&sm.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        // 128 TMEM columns: the 128 x 128 FP32 product of one tile
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(tc_smem(&sm.tmem_base)),
+                     "r"(H)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = sm.tmem_base;
+    const unsigned lane_addr = tmem + ((unsigned)(warp * 32) << 16);
+    const float b3 = a.master[a.b3];
+    const long ntiles = (a.N + TC_M - 1) / TC_M;
+    unsigned parity = 0;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long s = tile * TC_M + tid;
+        const bool valid = s < a.N;
+        // layer 1 on the FP32 cores, in k_mlp_pass's order: z1 = b1 + sum_d W1[h][d] x[d]
+        float z[H];
+#pragma unroll
+        for (int h = 0; h < H; ++h) z[h] = sm.b1[h];
+        for (int d = 0; d < D; ++d) {
+            const float xd = valid ? a.X[s * D + d] : 0.f;
+#pragma unroll
+            for (int h = 0; h < H; ++h) z[h] = fmaf(__bfloat162float(sm.W1t[d * H + h]), xd, z[h]);
+        }
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const float a1 = z[h] * sigm(z[h]);
+            const float hi = __uint_as_float(__float_as_uint(a1) & 0xffffe000u);  // exact in TF32
+            sm.Ahi[tc_idx(tid, h)] = hi;
+            sm.Alo[tc_idx(tid, h)] = a1 - hi;
+        }
+        // the tile's operands, written by every thread, become visible to the tensor core
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const unsigned ahi = tc_smem(sm.Ahi), alo = tc_smem(sm.Alo), bw = tc_smem(sm.W2f);
+            for (int k = 0; k < H / 8; ++k) {
+                const unsigned off = (unsigned)k * 2u * TC_LBO;  // K slice k: core matrices 2k, 2k+1
+                tc_mma(tmem, tc_desc(ahi + off), tc_desc(bw + off), k > 0);
+                tc_mma(tmem, tc_desc(alo + off), tc_desc(bw + off), true);
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             tc_smem(&sm.bar))
+                         : "memory");
+        }
+        bool done = false;
+        for (long it = 0; it < kTcSpin && !done; ++it) done = tc_try_wait(&sm.bar, parity);
+        parity ^= 1u;
+        if (__syncthreads_or(done ? 0 : 1)) {
+            if (tid == 0) atomicExch(err, 1);
+            break;
+        }
+        tc_fence_after();
+        float y = b3;
+#pragma unroll
+        for (int c = 0; c < H / 32; ++c) {
+            float v[32];
+            tc_ld32(lane_addr + (unsigned)(32 * c), v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                const float z2 = v[q] + sm.b2[32 * c + q];
+                y = fmaf(sm.w3[32 * c + q], z2 * sigm(z2), y);
+            }
+        }
+        if (valid) a.Y[s] = y;
+        // every thread's reads of the product precede the next tile's MMAs into it
+        tc_fence_before();
+        __syncthreads();
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(H) : "memory");
+    }
+}
+
 mra_status mfail(mra_status s, const std::string& msg) {
     mra::set_last_error(msg.c_str());
     return s;
@@ -302,6 +485,7 @@ struct mra_mlp {
     float *X = nullptr, *T = nullptr, *partial = nullptr, *grad = nullptr, *loss = nullptr;
     float *Xq = nullptr, *Yq = nullptr, *Gq = nullptr;
     int grid_train = 1;
+    int* tc_err = nullptr;  // bounded-wait status of the tensor-core forward pass
 };
 
 namespace {
@@ -402,6 +586,11 @@ mra_status mra_mlp_create(int32_t n_in, int32_t hidden, uint64_t seed, mra_mlp**
                                           : cudaFuncSetAttribute(k_mlp_pass<PREDICT_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
         if (e != cudaSuccess) return fail_free(mfail(MRA_ERR_CUDA, std::string("mra_mlp: smem attribute: ") + cudaGetErrorString(e)));
     }
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(TcSmem));
+        if (e != cudaSuccess) return fail_free(mfail(MRA_ERR_CUDA, std::string("mra_mlp: smem attribute: ") + cudaGetErrorString(e)));
+    }
     // Glorot-uniform weights from a host generator, zero biases
     std::vector<float> p(P, 0.f);
     std::mt19937_64 gen(seed);
@@ -427,6 +616,7 @@ mra_status mra_mlp_destroy(mra_mlp* n) {
     if (n->W1b) cudaFree(n->W1b);
     if (n->W2b) cudaFree(n->W2b);
     if (n->w3b) cudaFree(n->w3b);
+    if (n->tc_err) cudaFree(n->tc_err);
     if (n->stream) cudaStreamDestroy(n->stream);
     delete n;
     return MRA_OK;
@@ -516,18 +706,29 @@ mra_status mra_mlp_predict(mra_mlp* n, const float* x, int64_t N, float* y, floa
         MCU(cudaMalloc((void**)&n->Yq, (size_t)MAXN * sizeof(float)));
         MCU(cudaMalloc((void**)&n->Gq, (size_t)MAXN * n->D * sizeof(float)));
     }
+    if (!n->tc_err) MCU(cudaMalloc((void**)&n->tc_err, sizeof(int)));
     MCU(cudaMemcpyAsync(n->Xq, x, (size_t)N * n->D * sizeof(float), cudaMemcpyHostToDevice, n->stream));
     MlpArgs a = args_of(n, N, n->Xq);
     a.Y = n->Yq;
     a.G = n->Gq;
-    const long ntiles = (N + S - 1) / S;
-    const int grid = (int)std::min<long>(ntiles, 4L * n->sms);
-    if (dydx) k_mlp_pass<PREDICT_GRAD><<<grid, H, smem_bytes(PREDICT_GRAD, n->D), n->stream>>>(a);
-    else k_mlp_pass<PREDICT><<<grid, H, smem_bytes(PREDICT, n->D), n->stream>>>(a);
+    if (dydx) {
+        const long ntiles = (N + S - 1) / S;
+        const int grid = (int)std::min<long>(ntiles, 4L * n->sms);
+        k_mlp_pass<PREDICT_GRAD><<<grid, H, smem_bytes(PREDICT_GRAD, n->D), n->stream>>>(a);
+    } else {
+        // values only: the 128 x 128 layer on the tensor cores (tcgen05), 128 samples per tile
+        MCU(cudaMemsetAsync(n->tc_err, 0, sizeof(int), n->stream));
+        const long ntiles = (N + TC_M - 1) / TC_M;
+        const int grid = (int)std::min<long>(ntiles, n->sms);
+        k_mlp_forward_tc<<<grid, TC_M, sizeof(TcSmem), n->stream>>>(a, n->tc_err);
+    }
     MCU(cudaGetLastError());
     MCU(cudaMemcpyAsync(y, n->Yq, (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
     if (dydx) MCU(cudaMemcpyAsync(dydx, n->Gq, (size_t)N * n->D * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+    int tc_err = 0;
+    if (!dydx) MCU(cudaMemcpyAsync(&tc_err, n->tc_err, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
     MCU(cudaStreamSynchronize(n->stream));
+    if (tc_err) return mfail(MRA_ERR_TIMEOUT, "mra_mlp_predict: the tensor-core product did not complete in time");
     return MRA_OK;
 }
 

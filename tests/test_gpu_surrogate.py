@@ -28,6 +28,23 @@ def test_forward_matches_oracle():
     net.close()
 
 
+def test_tensor_core_forward_many_tiles():
+    # values only: the 128 x 128 layer runs on tcgen05 (128-sample tiles, more
+    # tiles than SMs, a partial last tile); with input gradients the same network
+    # runs on the FP32 cores -- the two agree to FP32 rounding, and both match the
+    # oracle
+    net = Surrogate(N_IN, seed=11)
+    x, _ = data(5, 40000)
+    y_tc = net.predict(x)
+    y_fp32, _ = net.predict(x, with_grad=True)
+    y_ref, _ = mo.forward(net.params(), x, N_IN)
+    np.testing.assert_allclose(y_tc, y_fp32, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(y_tc, y_ref, rtol=1e-4, atol=1e-5)
+    # a second call reuses the same buffers and barrier phases
+    np.testing.assert_array_equal(net.predict(x[:333]), y_tc[:333])
+    net.close()
+
+
 def test_parameter_gradient_matches_oracle():
     net = Surrogate(N_IN, seed=2)
     x, t = data(1, 203)     # not a multiple of the 16-sample tile
