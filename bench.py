@@ -87,6 +87,9 @@ def parse_args():
     p.add_argument("--shard", action="store_true",
                    help="with N ranks: one log-likelihood per step split over the ranks by sub-trees "
                         "(strong scaling; shard.py) instead of N independent replicas")
+    p.add_argument("--surrogate-forward", action="store_true",
+                   help="instead of the log-likelihood line: the surrogate network's prediction on 65,536 "
+                        "parameter vectors, values only (tcgen05 kernel) and with input gradients (FP32 cores)")
     p.add_argument("--no-compare", action="store_true",
                    help="skip timing the other precision on the same inputs")
     return p.parse_args()
@@ -708,6 +711,32 @@ def shard_arm(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def surrogate_forward_arm(args):
+    """The surrogate's batched prediction (19 -> 128 -> 128 -> 1, 65,536 parameter vectors per call): values
+    only, whose 128 x 128 layer runs on the tensor cores (tcgen05), and values with input gradients on the FP32
+    cores.  Per call, with the host copies of the inputs and results, CUDA-stream wall clock after warm-up."""
+    from nonstationary_mra_b200.fit import Surrogate
+    net = Surrogate(19, seed=1)
+    x = np.random.default_rng(0).standard_normal((65536, 19)).astype(np.float32)
+    for _ in range(max(args.warmup, 1)):
+        y = net.predict(x)
+    steps = max(args.steps, 1) * 4
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        y = net.predict(x)
+    t1 = time.perf_counter()
+    for _ in range(steps):
+        y2, _ = net.predict(x, with_grad=True)
+    t2 = time.perf_counter()
+    net.close()
+    print(json.dumps({"metric": "surrogate predictions/s (65,536 per call, host copies included)",
+                      "values_tcgen05": {"ms_per_call": 1e3 * (t1 - t0) / steps,
+                                         "predictions_per_s": 65536 * steps / (t1 - t0)},
+                      "values_and_input_gradients_fp32": {"ms_per_call": 1e3 * (t2 - t1) / steps,
+                                                          "predictions_per_s": 65536 * steps / (t2 - t1)},
+                      "max_abs_difference": float(np.max(np.abs(y - y2))), "steps": steps}))
+
+
 def main():
     args = parse_args()
     if args.mixed_report:
@@ -724,6 +753,9 @@ def main():
         return
     if args.sweep:
         sweep_arm(args)
+        return
+    if args.surrogate_forward:
+        surrogate_forward_arm(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
