@@ -141,6 +141,10 @@ typedef struct {
     int32_t timed_level[MRA_MAX_TIMED];  /* tree level for per-level kernels, else -1 */
     double timed_ms[MRA_MAX_TIMED];      /* device time of each launch (CUDA events) */
     double timed_flop[MRA_MAX_TIMED];    /* algorithmic FLOPs of each launch          */
+    double timed_ms_cov[MRA_MAX_TIMED];  /* of timed_ms, the device time of the prior
+                                            level's covariance-block launches (the rest
+                                            is its region launches); 0 for other kinds,
+                                            -1 where some went untimed */
 } mra_stats;
 
 typedef struct mra_ctx mra_ctx;

@@ -156,7 +156,8 @@ class Context:
         out = {k: getattr(s, k) for k, _ in capi.mra_stats._fields_ if not k.startswith("timed_")}
         n = s.n_timed
         out["launches"] = [{"kernel": capi.KERNEL_NAMES.get(s.timed_kind[i], "?"), "level": s.timed_level[i],
-                            "ms": s.timed_ms[i], "flop": s.timed_flop[i]} for i in range(n)]
+                            "ms": s.timed_ms[i], "flop": s.timed_flop[i], "ms_cov": s.timed_ms_cov[i]}
+                           for i in range(n)]
         return out
 
     # ---- sub-tree sharding (include/mra_b200.h: mra_shard_*) ----

@@ -56,7 +56,8 @@ class mra_stats(C.Structure):
                 ("bytes_device", C.c_uint64),
                 ("bad_region", C.c_int64), ("kernel_launches", C.c_int32), ("graph_replays", C.c_int32),
                 ("n_timed", C.c_int32), ("timed_kind", C.c_int32 * 40), ("timed_level", C.c_int32 * 40),
-                ("timed_ms", C.c_double * 40), ("timed_flop", C.c_double * 40)]
+                ("timed_ms", C.c_double * 40), ("timed_flop", C.c_double * 40),
+                ("timed_ms_cov", C.c_double * 40)]
 
 class mra_opt_config(C.Structure):
     _fields_ = [("rho_begin", C.c_double), ("rho_end", C.c_double), ("npt", C.c_int32), ("max_evals", C.c_int32)]

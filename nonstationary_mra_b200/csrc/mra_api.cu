@@ -60,6 +60,13 @@ struct mra_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8]{};
     cudaEvent_t tev[2 * MRA_MAX_TIMED]{};  // start/stop of every launch
+    // start/stop of each covariance-block launch of the prior levels, and the
+    // timed launch (index into tev pairs) that each belongs to
+    static constexpr int kMaxCovTimed = 64;
+    cudaEvent_t cev[2 * kMaxCovTimed]{};
+    int cov_owner[kMaxCovTimed]{};
+    int n_cov = 0;
+    bool cov_overflow = false;
     struct Launch {
         int kind, level;
         double flop;
@@ -84,6 +91,7 @@ struct mra_ctx {
     cudaGraphExec_t graph_pred_exec = nullptr;
     int graph_timed[2] = {0, 0};     // timed stages of the log-likelihood / prediction graph
     int graph_launches[2] = {0, 0};  // kernels launched by each
+    int graph_cov[2] = {0, 0};       // timed covariance-block launches of each
     double* d_theta = nullptr;  // 16 doubles
     double* d_weights[3]{};
     long nb[3]{};
@@ -120,6 +128,8 @@ struct mra_ctx {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : tev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : cev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
         for (auto& b : bufs) cudaFree(b.p);
@@ -280,6 +290,7 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     const long rr = (long)c->r * c->r;
     int i = 0, launched = 0;
     c->timed_plan.clear();
+    CovTiming cov{c->cev, mra_ctx::kMaxCovTimed, 0, capturing, false};
     for (size_t pi = 0; pi < c->plan.size(); ++pi) {
         const auto& l = c->plan[pi];
         if (c->eval_phase != 0) {
@@ -296,10 +307,14 @@ mra_status run_eval(mra_ctx* c, bool predict) {
                               const_cast<double*>(td.pts.beta), const_cast<double*>(td.pts.t2), st);
                 launched += 1;
                 break;
-            case MRA_KERNEL_PRIOR_LEVEL:
-                if (mixed && c->mixed_prior32) launched += launch_prior_level<float>(c->geom, tf, l.level, c->grid, st);
-                else launched += launch_prior_level<double>(c->geom, td, l.level, c->grid, st);
+            case MRA_KERNEL_PRIOR_LEVEL: {
+                const int u0 = cov.used;
+                if (mixed && c->mixed_prior32)
+                    launched += launch_prior_level<float>(c->geom, tf, l.level, c->grid, st, &cov);
+                else launched += launch_prior_level<double>(c->geom, td, l.level, c->grid, st, &cov);
+                for (int k = u0; k < cov.used; ++k) c->cov_owner[k] = i;
                 break;
+            }
             case MRA_KERNEL_FINEST:
                 if (mixed && c->mixed_prior32 != c->mixed_finest32) {
                     // the finest level runs in the other precision: its ancestors' factors follow it
@@ -357,6 +372,8 @@ mra_status run_eval(mra_ctx* c, bool predict) {
     }
     CU(cudaGetLastError());
     c->n_timed = i;
+    c->n_cov = cov.used;
+    c->cov_overflow = cov.overflow;
     c->last_launches = launched;
     return MRA_OK;
 }
@@ -382,6 +399,7 @@ mra_status finish_eval(mra_ctx* c) {
         s.timed_level[i] = in_plan ? c->plan[pi].level : -1;
         s.timed_flop[i] = in_plan ? c->plan[pi].flop : c->flop_predict_launch;
         s.timed_ms[i] = ms;
+        s.timed_ms_cov[i] = 0;
         s.ms_total += ms;
         if (kind == MRA_KERNEL_FIELDS) s.ms_fields += ms;
         else if (kind == MRA_KERNEL_PRIOR_LEVEL) s.ms_prior += ms;
@@ -389,6 +407,14 @@ mra_status finish_eval(mra_ctx* c) {
         else if (kind == MRA_KERNEL_PREDICT) s.ms_predict += ms;
         else s.ms_posterior += ms;
     }
+    for (int k = 0; k < c->n_cov; ++k) {
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, c->cev[2 * k], c->cev[2 * k + 1]));
+        if (c->cov_owner[k] < c->n_timed) s.timed_ms_cov[c->cov_owner[k]] += ms;
+    }
+    if (c->cov_overflow)  // some covariance launches went untimed: the split is unknown
+        for (int i = 0; i < c->n_timed; ++i)
+            if (s.timed_kind[i] == MRA_KERNEL_PRIOR_LEVEL) s.timed_ms_cov[i] = -1;
     s.d = d;
     s.loglik = -0.5 * (d + (double)c->n_obs * std::log(2 * 3.14159265359));
     s.flop_last = c->flop_loglik;
@@ -640,6 +666,8 @@ mra_status mra_create(const mra_structure* s, const mra_model* m, int32_t precis
     for (auto& e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "event creation failed"));
     for (auto& e : c->tev)
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "event creation failed"));
+    for (auto& e : c->cev)
         if (cudaEventCreate(&e) != cudaSuccess) return bail(fail(MRA_ERR_CUDA, "event creation failed"));
 
     // host-side tables
@@ -933,6 +961,7 @@ mra_status mra_loglik(mra_ctx* c, double* d_out, double* ll_out) {
         CU(cudaGraphLaunch(c->graph_exec, c->stream));
         c->stats.graph_replays++;
         c->n_timed = c->graph_timed[0];
+        c->n_cov = c->graph_cov[0];
         c->last_launches = c->graph_launches[0];
     } else {
         mra_status s = run_eval(c, false);
@@ -954,6 +983,7 @@ mra_status mra_predict(mra_ctx* c, double* mean, double* var) {
         CU(cudaGraphLaunch(c->graph_pred_exec, c->stream));
         c->stats.graph_replays++;
         c->n_timed = c->graph_timed[1];
+        c->n_cov = c->graph_cov[1];
         c->last_launches = c->graph_launches[1];
     } else {
         mra_status s = run_eval(c, true);
@@ -991,6 +1021,7 @@ mra_status capture_one(mra_ctx* c, bool predict, cudaGraph_t* graph, cudaGraphEx
     *graph = g;
     c->graph_timed[predict ? 1 : 0] = c->n_timed;
     c->graph_launches[predict ? 1 : 0] = c->last_launches;
+    c->graph_cov[predict ? 1 : 0] = c->n_cov;
     return MRA_OK;
 }
 

@@ -977,7 +977,11 @@ void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const
     k_fields<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, fp, c0, c1, c2, n, s2, beta, t2);
 }
 template <typename T>
-int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st) {
+int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st, CovTiming* tm) {
+    auto mark = [&](cudaEvent_t e) {
+        if (tm->capturing) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+        else cudaEventRecord(e, st);
+    };
     const long cnt = level_count(t.J, m);
     const long per_region = (long)(m + 1) * t.r * t.r;
     long per = t.cbuf_elems / per_region;  // regions whose blocks fit the buffer at once
@@ -987,7 +991,11 @@ int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cuda
         const long n = cnt - loc0 < per ? cnt - loc0 : per;
         const long nb = n * (m + 1);
         const long cov_grid = (long)grid * 16;  // 16 per region-kernel slot: 32 CTAs per SM
+        const bool timed = tm && tm->used < tm->cap;
+        if (tm && !timed) tm->overflow = true;
+        if (timed) mark(tm->ev[2 * tm->used]);
         launch_cov_level<T>(g, t, m, loc0, n, (unsigned)(nb < cov_grid ? nb : cov_grid), st);
+        if (timed) mark(tm->ev[2 * tm->used++ + 1]);
         k_prior_level<T><<<(unsigned)(n < grid ? n : grid), kThreads, sizeof(LaSmem<T>), st>>>(g, t, m, loc0, n,
                                                                                                 t.cbuf);
         launches += 2;
@@ -1059,7 +1067,7 @@ cudaError_t prepare_kernels() {
 }
 
 #define MRA_INSTANTIATE(T)                                                                                   \
-    template int launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t);             \
+    template int launch_prior_level<T>(const Geom&, const DevTree<T>&, int, int, cudaStream_t, CovTiming*); \
     template int launch_finest_group<T>(const Geom&, const DevTree<T>&, int, bool, cudaStream_t);           \
     template void launch_posterior_level<T>(const Geom&, const DevTree<T>&, int, int, bool, cudaStream_t);  \
     template void launch_predict<T>(const Geom&, const DevTree<T>&, int, cudaStream_t);                     \

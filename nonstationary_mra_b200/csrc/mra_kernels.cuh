@@ -128,10 +128,20 @@ cudaError_t set_gemm_tiles(const int nw[3]);
 
 void launch_fields(const Geom& g, const FieldParams& fp, const double* c0, const double* c1, const double* c2,
                    long n, double* s2, double* beta, double* t2, cudaStream_t st);
+// Events recorded around each covariance-block launch of a prior level, so
+// that the caller can split the level's device time between the covariance
+// launches and the region launches.
+struct CovTiming {
+    cudaEvent_t* ev;  // two per launch: before and after
+    int cap;          // launches that can be timed
+    int used;         // launches timed so far
+    bool capturing;   // record as external nodes of the graph being captured
+    bool overflow;    // a launch went untimed (cap reached)
+};
 // Covariance-block launches and region launches of one prior level, in chunks
 // of regions whose blocks fit t.cbuf; returns the number of kernels launched.
 template <typename T>
-int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st);
+int launch_prior_level(const Geom& g, const DevTree<T>& t, int m, int grid, cudaStream_t st, CovTiming* tm = nullptr);
 // The finest groups; returns the number of kernels launched (1).
 template <typename T>
 int launch_finest_group(const Geom& g, const DevTree<T>& t, int grid, bool keep, cudaStream_t st);

@@ -162,6 +162,12 @@ def test_graph_replay_and_theta_updates():
     d_ref, _ = oracle.loglik(ost, omd)
     assert d2 != d0 and abs(d2 - d_ref) <= LL_RTOL * max(1.0, abs(d_ref))
     assert ctx.stats()["graph_replays"] >= 2
+    # each prior level's time splits into its covariance-block launches and its
+    # region launches, also when replayed from the graph
+    prior = [l for l in ctx.stats()["launches"] if l["kernel"] == "prior_level"]
+    assert len(prior) == st.M - 1
+    assert all(0 < l["ms_cov"] < l["ms"] for l in prior), prior
+    assert all(l["ms_cov"] == 0 for l in ctx.stats()["launches"] if l["kernel"] != "prior_level")
     ctx.close()
 
 

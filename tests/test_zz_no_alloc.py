@@ -74,3 +74,19 @@ def test_static_rejects_requests_beyond_its_scratch():
         _call_static(md, dict(), big, None, True, out)
     assert e.value.status == capi.MRA_ERR_ARG
     assert "MRA_STATIC_MAX_POINTS" in str(e.value)
+
+
+def test_static_rejects_a_model_the_allocating_entry_point_rejects():
+    # the same model check as mra_eval_covariance: a zero basis length would
+    # otherwise give inf/NaN covariances without an error
+    torch = pytest.importorskip("torch")
+    api.set_device(0)
+    st, md, _ = refio.load_case(CASE, mode="likelihood")
+    assert md.nonstationary
+    md.basis_len = 0.0
+    pts = _device(st.obs[:, :8], torch)
+    out = torch.zeros((8, 8), dtype=torch.float64, device="cuda")
+    with pytest.raises(capi.MRAError) as e:
+        _call_static(md, dict(), pts, None, True, out)
+    assert e.value.status == capi.MRA_ERR_ARG
+    assert "basis length" in str(e.value)
