@@ -100,6 +100,8 @@ RANDOM_CASES = [
     (6, 4, 5, 16, 3000, 200, True, 3, True),     # finest work items both batched and split; children up to 230
     (8, 4, 5, 16, 1200, 60, False, 3, True),     # finest children of about 5 observations: one warp per child
     (9, 4, 5, 12, 1500, 50, True, 1, True),      # clustered: per-warp, grouped and per-child paths side by side
+    (10, 4, 3, 128, 3000, 40, True, 3, True),    # r = 120 (12 x 10 knots): factors and tiles beyond 64 rows
+    (11, 2, 4, 96, 2000, 30, False, 1, True),    # r = 90, J = 2
 ]
 
 
