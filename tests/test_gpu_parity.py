@@ -102,6 +102,8 @@ RANDOM_CASES = [
     (9, 4, 5, 12, 1500, 50, True, 1, True),      # clustered: per-warp, grouped and per-child paths side by side
     (10, 4, 3, 128, 3000, 40, True, 3, True),    # r = 120 (12 x 10 knots): factors and tiles beyond 64 rows
     (11, 2, 4, 96, 2000, 30, False, 1, True),    # r = 90, J = 2
+    (12, 4, 3, 196, 4000, 40, False, 3, True),   # r = 196: blocked factorization, inverse by triangular solve
+    (13, 2, 3, 256, 3000, 30, True, 1, True),    # r = 256, the largest supported
 ]
 
 
